@@ -1,0 +1,358 @@
+"""Benchmark of the B200 engine for BSim's SGSim LIF step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config NAME] [--impl ours|reference]
+
+A step is one simulation cycle (dt = 0.1 ms) of the whole network. The default
+workload is the 1e6-neuron CUBA network (100 populations x 10,000 LIF_brian
+neurons, ~1.19e9 synapses, ~500 Hz, delays U{1..6} steps), built on the device
+by the seeded generator. Metric: synaptic events per second (one event = one
+synapse delivering one spike), plus the realtime factor (simulated seconds per
+wall second). With N > 1 (torchrun, one process per GPU) every rank simulates
+its own replica (a different seed): the networks are independent, so there is
+no data-path collective, only a barrier and a max over ranks of the timing.
+
+--impl reference times the reference's own CPU simulator (oracle/_ref, built
+from its sources) on a scaled-down replica of the same workload.
+"""
+import argparse
+import json
+import os
+import signal
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DT = 1.0e-4
+HBM_FALLBACK_GBS = 6650.0
+# Algorithmic bytes per unit of work of one step ("Roofline"):
+BYTES_PER_NEURON_STEP = 52.0   # read/write v, i_E, i_I, refrac (32), v_tmp (4), read+clear E/I input (16)
+BYTES_PER_EVENT = 8.0          # int32 target + fp32 weight of one delivered synapse
+BYTES_PER_SPIKE = 8.0          # fired id written once, read once
+
+
+def workload(name, seed):
+    from bsim_b200 import workloads as W
+    if name == "plain_1m":
+        specs, _ = W.plain_1m(seed)
+        desc = "100 x 10,000 LIF_brian CUBA, ~500 Hz, delays U{1..6}, p=0.1 chain + 20% remote"
+    elif name == "standard_cpu":
+        specs, _ = W.standard_cpu(seed)
+        desc = "10 x 1,000 LIF_brian CUBA, ~100 Hz, delays U{1..6}"
+    elif name == "dense_1m":
+        specs, _ = W.dense_1m(seed)
+        desc = "50 x 20,000 LIF_brian CUBA, ~2 kHz, delays U{1..50}"
+    elif name.startswith("batched"):
+        k = int(name.split("_")[1]) if "_" in name else 256
+        specs, _ = W.batched(k, seed)
+        desc = "%d independent CUBA nets, populations U{5..40} x neurons U{500..8000}" % k
+    else:
+        raise SystemExit("unknown config " + name)
+    return specs, desc
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.send_signal(signal.SIGTERM)
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        if self.path and os.path.exists(self.path):
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9:
+                    rows.append(f)
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())
+                if any(r[3].replace(".", "").isdigit() for r in rows) else None}
+
+
+def measured_hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        try:
+            return float(json.load(open(p))["hbm_gbs"]), "measured"
+        except (ValueError, KeyError):
+            pass
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+def profiled_traffic(config):
+    """DRAM bytes per launch of the step kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        v = d.get(config)
+        if isinstance(v, dict):
+            return v.get("bytes_per_launch")
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines (oracle/_ref: the reference's own simulator, else the oracle port)
+# ---------------------------------------------------------------------------
+def replica_net(spec, pop_size):
+    """Scaled-down replica of a generated workload, in the reference API's terms."""
+    import bsim_b200 as B
+    from bsim_b200 import workloads as W
+    rs = W.scaled(spec, pop_size)
+    g = B.gen_host(rs)
+    dt = np.float32(DT)
+    net = dict(params=g["params"].astype(np.float64), pop_size=np.full(rs.n_pop, rs.pop_size, np.int64),
+               pop_tau=np.tile([rs.tau_syn_E, rs.tau_syn_I], (rs.n_pop, 1)).astype(np.float64),
+               src=g["src"], dst=g["dst"], weight=g["weight"].astype(np.float64),
+               delay=(g["delay_steps"].astype(np.float32) * dt).astype(np.float64),
+               type=(g["weight"] < 0).astype(np.uint8), dt=float(dt))
+    return rs, g, net
+
+
+def cpu_baseline(spec, steps, budget_s=20.0):
+    """Times the reference simulator (or the oracle port) on a replica sized so
+    that the run takes about budget_s seconds. Returns (events/s, dict)."""
+    from oracle import oracle
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import netio
+    S_full = spec.n_pop * (spec.pop_size ** 2) * spec.p_conn * 1.2
+    ref = oracle.ref_available("f32")
+    # the reference walks every synapse every step (~20 ns each on one core)
+    pop = int(spec.pop_size * min(1.0, np.sqrt(budget_s / (20e-9 * S_full * steps))))
+    pop = max(pop, 20)
+    rs, g, net = replica_net(spec, pop)
+    orc = oracle.run(g["params"], g["src"], g["dst"], g["weight"], g["delay_steps"], np.float32(DT), steps)
+    events = int(orc["events_per_step"].sum())
+    if ref:
+        with tempfile.TemporaryDirectory() as d:
+            netio.write_net(os.path.join(d, "net.bin"), net, steps, 0)
+            r = oracle.run_reference(os.path.join(d, "net.bin"), os.path.join(d, "out.bin"), "f32",
+                                     record=False, n=g["params"].shape[0], n_rec=0)
+        secs, kind = r["seconds"], "reference"
+    else:
+        t0 = time.perf_counter()
+        oracle.run(g["params"], g["src"], g["dst"], g["weight"], g["delay_steps"], np.float32(DT), steps)
+        secs, kind = time.perf_counter() - t0, "port"
+    sample = ("%s: %d steps of a %d x %d replica (%d synapses) of the same generator; 1 thread; "
+              "events/s is independent of the replica size at a fixed rate" %
+              ("reference STSim float build (oracle/_ref)" if kind == "reference" else "oracle port",
+               steps, rs.n_pop, rs.pop_size, len(g["src"])))
+    return events / secs, dict(kind=kind, sample=sample, seconds=secs, events=events,
+                               rtf=steps * DT / secs, replica_synapses=int(len(g["src"])))
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    specs, desc = workload(args.config, 1)
+    total = args.steps + args.warmup
+    try:
+        eps, info = cpu_baseline(specs[0], total, budget_s=90.0)
+    except Exception as ex:  # reference missing or failed
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU run failed: %s" % ex}))
+        return
+    line = {"impl": "reference", "metric": "synaptic events/s", "value": eps, "unit": "events/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * info["seconds"] / total, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+            "config": {"workload": args.config + ": " + desc, "sample": info["sample"]},
+            "realtime_factor": info["rtf"],
+            "cpu_baseline": {"value": eps, "unit": "events/s", "cores": 1, "kind": info["kind"],
+                             "sample": info["sample"]},
+            "e2e": {"value": eps, "unit": "events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# Our arm
+# ---------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10000)
+    ap.add_argument("--warmup", type=int, default=200)
+    ap.add_argument("--config", default="plain_1m")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--delivery", default="push", choices=["push", "pull"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import bsim_b200 as B
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    specs, desc = workload(args.config, 1 + rank)
+    deliv = B.DELIVERY_PULL if args.delivery == "pull" else B.DELIVERY_PUSH
+    t_build = time.perf_counter()
+    eng = B.Engine.generated(specs, DT, opts=B.options(device=local, delivery=deliv, graph_steps=100))
+    t_build = time.perf_counter() - t_build
+    info = eng.info()
+    N, S = info.n_neurons, info.n_synapses
+
+    eng.run(args.warmup)
+    stream = torch.cuda.ExternalStream(eng.stream(), device=local)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    i0 = eng.info()
+    fc0 = eng.fire_count().astype(np.int64)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        eng.run_async(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+    eng.sync()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    i1 = eng.info()
+    events = int(i1.events_total - i0.events_total)
+    spikes = int((eng.fire_count().astype(np.int64) - fc0).sum())
+    tot = torch.tensor([ms, float(events), float(spikes), float(N)], dtype=torch.float64, device="cuda")
+    if dist:
+        mx = tot.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = tot.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        ms_max, events_all, spikes_all, n_all = float(mx[0]), float(sm[1]), float(sm[2]), float(sm[3])
+    else:
+        ms_max, events_all, spikes_all, n_all = ms, float(events), float(spikes), float(N)
+    value = events_all / (ms_max / 1e3)
+    rtf = args.steps * DT / (ms_max / 1e3)
+    ms_step = ms_max / args.steps
+
+    # end to end through the C ABI with host buffers: upload the neuron state,
+    # run the steps recording every spike, read the raster and the counts back
+    st = eng.state()
+    v, ie, ii, rf = st["v"], st["i_E"], st["i_I"], st["refrac"]
+    e2e_steps = args.steps
+    cap = int(max(4 * spikes, 1024))
+    eng.record(e2e_steps, cap)  # allocates the recording buffers (drops the captured graph)
+    eng.run(100)                # re-captures the graph with recording enabled (not timed)
+    eng.record(e2e_steps, cap)  # re-arms the recording only
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ia = eng.info()
+    t0 = time.perf_counter()
+    eng.write_state(v, ie, ii, rf)
+    eng.run(e2e_steps)
+    raster = eng.raster()
+    counts = eng.fire_count()
+    t_e2e = time.perf_counter() - t0
+    ib = eng.info()
+    ev_e2e = float(ib.events_total - ia.events_total)
+    spk_e2e = sum(len(r) for r in raster)
+    t_e2e_max = t_e2e
+    ev_all_e2e = ev_e2e
+    if dist:
+        x = torch.tensor([t_e2e, ev_e2e], dtype=torch.float64, device="cuda")
+        mx = x.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = x.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        t_e2e_max, ev_all_e2e = float(mx[0]), float(sm[1])
+    e2e = {"value": ev_all_e2e / t_e2e_max, "unit": "events/s",
+           "h2d_bytes_per_step": 16.0 * N / e2e_steps,
+           "d2h_bytes_per_step": (4.0 * spk_e2e + 8.0 * (e2e_steps + 1) + 4.0 * len(counts)) / e2e_steps,
+           "realtime_factor": e2e_steps * DT / t_e2e_max,
+           "path": "bsim_write_state (H2D) + bsim_run with spike recording + bsim_read_raster + "
+                   "bsim_read_fire_count (D2H), wall clock"}
+
+    peak, peak_kind = measured_hbm_peak()
+    alg_bytes = (BYTES_PER_NEURON_STEP * N + BYTES_PER_EVENT * events / args.steps +
+                 BYTES_PER_SPIKE * spikes / args.steps)
+    achieved = alg_bytes / (ms / args.steps / 1e3) / 1e9
+    traffic = profiled_traffic(args.config)
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
+            if peak_kind == "measured" else "fallback 6.65 TB/s",
+            "kernel": "step_kernel<EXACT> (fused LIF update + %s delivery), one launch per step" % args.delivery,
+            "alg_bytes_per_launch": alg_bytes}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            eps, ci = cpu_baseline(specs[0], 300)
+            cpu = {"value": eps, "unit": "events/s", "cores": 1, "kind": ci["kind"], "sample": ci["sample"],
+                   "realtime_factor_of_sample": ci["rtf"]}
+        except Exception as ex:
+            cpu = {"value": None, "unit": "events/s", "cores": 1, "kind": "unavailable", "sample": str(ex)}
+
+    if rank == 0:
+        line = {"metric": "synaptic events/s", "value": value, "unit": "events/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic: seeded generator, networks built on the device",
+                "config": {"workload": args.config + ": " + desc, "neurons_per_gpu": N, "synapses_per_gpu": S,
+                           "delivery": args.delivery, "accumulate": "exact int64",
+                           "parallelism": "replicas x%d (independent networks, no collective)" % world,
+                           "l2": "inputs larger than L2 (%.1f GB of synapse rows per GPU)" % (S * 8 / 1e9),
+                           "build_seconds": t_build},
+                "realtime_factor": rtf, "spikes_per_step": spikes_all / args.steps / world,
+                "events_per_step": events_all / args.steps / world,
+                "mean_rate_hz": spikes_all / n_all / (args.steps * DT),
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
+                "gpu_launches": args.steps}
+        print(json.dumps(line))
+    eng.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1115 @@
+// Engine construction (host arrays or on-device generation), the run loop and
+// the C ABI entry points declared in include/bsim_b200.h.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include <cub/device/device_scan.cuh>
+
+#include "engine.h"
+#include "netgen.h"
+
+namespace bsim {
+
+cudaError_t launch_step(Engine &e);
+cudaError_t launch_record_flush(Engine &e);
+cudaError_t step_occupancy(int block, int accumulate, int *blocks_per_sm);
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                    \
+    do {                                                                                            \
+        cudaError_t _e = (call);                                                                    \
+        if (_e != cudaSuccess) return fail(BSIM_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(_e)); \
+    } while (0)
+
+template <typename T>
+static int dalloc(Engine &e, T **p, size_t count)
+{
+    size_t bytes = sizeof(T) * (count ? count : 1);
+    cudaError_t st = cudaMalloc((void **)p, bytes);
+    if (st != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(BSIM_ERR_NOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(st));
+    }
+    e.allocs.push_back(*p);
+    e.device_bytes += (int64_t)bytes;
+    return BSIM_OK;
+}
+
+#define TRY(x)                      \
+    do {                            \
+        int _rc = (x);              \
+        if (_rc != BSIM_OK) return _rc; \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// LIFENeuron::reset (src/neuron/lif/LIFENeuron.cpp:68-112), fp32, on the host
+// with the C library's expf, exactly as the reference's float build folds it.
+// ---------------------------------------------------------------------------
+struct Folded {
+    float Cm, CE, CI, C_E, C_I, v_thresh, v_reset;
+    int32_t refrac_time;
+    float v_tmp, v_init;
+};
+
+static Folded fold_lif(const float *p, float dt)
+{
+    const float ZERO = 1e-10f;  // src/utils/constant.h:20
+    const float v_init = p[0], v_rest = p[1], v_reset = p[2], cm = p[3], tau_m = p[4];
+    const float tau_refrac = p[5], tau_syn_E = p[6], tau_syn_I = p[7], v_thresh = p[8], i_offset = p[9];
+    Folded f;
+    float rm = 1.0f;
+    if (fabsf(cm) > ZERO) rm = tau_m / cm;
+    f.Cm = tau_m > 0 ? expf(-dt / tau_m) : 0.0f;
+    f.CE = tau_syn_E > 0 ? expf(-dt / tau_syn_E) : 0.0f;
+    f.CI = tau_syn_I > 0 ? expf(-dt / tau_syn_I) : 0.0f;
+    float v_tmp = i_offset * rm + v_rest;
+    v_tmp = v_tmp * (1.0f - f.Cm);
+    float C_E = rm * tau_syn_E / (tau_syn_E - tau_m);
+    float C_I = rm * tau_syn_I / (tau_syn_I - tau_m);
+    f.C_E = C_E * (f.CE - f.Cm);
+    f.C_I = C_I * (f.CI - f.Cm);
+    f.v_thresh = v_thresh;
+    f.v_reset = v_reset;
+    f.refrac_time = (int32_t)(tau_refrac / dt);
+    f.v_tmp = v_tmp;
+    f.v_init = v_init;
+    return f;
+}
+
+// Smallest k with 2^k >= x (x >= 1).
+static int ceil_log2_i64(int64_t x)
+{
+    int k = 0;
+    while (k < 63 && ((int64_t)1 << k) < x) k++;
+    return k;
+}
+
+// Fixed-point exponent of one network: every per-target E or I sum of
+// |w| * 2^qexp stays below 2^61, so int64 accumulation cannot overflow.
+static int32_t choose_qexp(int64_t max_indeg, float max_abs_w)
+{
+    if (max_indeg <= 0 || !(max_abs_w > 0.0f)) return 0;
+    int e_w = 0;
+    frexpf(max_abs_w, &e_w);  // max_abs_w < 2^e_w
+    int q = 61 - ceil_log2_i64(max_indeg) - e_w;
+    if (q > 126) q = 126;
+    if (q < -126) q = -126;
+    return q;
+}
+
+static uint32_t f2u(float f)
+{
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    return u;
+}
+
+static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab);
+
+static int init_device(Engine &e, const bsim_options *opt)
+{
+    if (opt) e.opt = *opt;
+    else bsim_options_default(&e.opt);
+    e.device = e.opt.device;
+    CK(cudaSetDevice(e.device));
+    CK(cudaDeviceGetAttribute(&e.sm_count, cudaDevAttrMultiProcessorCount, e.device));
+    CK(cudaStreamCreateWithFlags(&e.stream, cudaStreamNonBlocking));
+    if (e.opt.accumulate == BSIM_ACC_ORDERED) e.opt.delivery = BSIM_DELIVERY_PULL;
+    if (e.opt.accumulate == BSIM_ACC_ORDERED || e.opt.delivery != BSIM_DELIVERY_PUSH) e.opt.build_pull = 1;
+    return BSIM_OK;
+}
+
+static void free_engine(Engine *e)
+{
+    if (!e) return;
+    cudaSetDevice(e->device);
+    if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    for (void *p : e->allocs) cudaFree(p);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+// ---------------------------------------------------------------------------
+// Host-array construction.
+// ---------------------------------------------------------------------------
+static int create_from_arrays(const float *params, int64_t n, const int32_t *pop, const int32_t *inst,
+                              const int32_t *src, const int32_t *dst, const float *weight,
+                              const int32_t *delay, int64_t s, float dt, const bsim_options *opt, Engine **out)
+{
+    if (!params || n <= 0 || s < 0 || (s > 0 && (!src || !dst || !weight || !delay)) || !(dt > 0) || !out)
+        return fail(BSIM_ERR_ARG, "bsim_create: invalid arguments");
+    if (n > (int64_t)INT32_MAX - 64) return fail(BSIM_ERR_LIMIT, "bsim_create: more than 2^31-64 neurons");
+    int32_t D = 1, n_inst = 1, n_pops = 1;
+    for (int64_t i = 0; i < n; i++) {
+        if (inst && inst[i] < 0) return fail(BSIM_ERR_ARG, "bsim_create: negative instance id");
+        if (pop && pop[i] < 0) return fail(BSIM_ERR_ARG, "bsim_create: negative population id");
+        if (inst) n_inst = std::max(n_inst, inst[i] + 1);
+        if (pop) n_pops = std::max(n_pops, pop[i] + 1);
+    }
+    for (int64_t k = 0; k < s; k++) {
+        if (src[k] < 0 || src[k] >= n || dst[k] < 0 || dst[k] >= n)
+            return fail(BSIM_ERR_ARG, "bsim_create: synapse " + std::to_string(k) + " has a neuron id out of range");
+        if (delay[k] < 1 || delay[k] > BSIM_MAX_DELAY)
+            return fail(BSIM_ERR_DELAY, "bsim_create: synapse " + std::to_string(k) + " has delay " +
+                                            std::to_string(delay[k]) + " steps (allowed 1.." +
+                                            std::to_string(BSIM_MAX_DELAY) + ")");
+        if (inst && inst[src[k]] != inst[dst[k]])
+            return fail(BSIM_ERR_ARG, "bsim_create: synapse " + std::to_string(k) + " joins two instances");
+        D = std::max(D, delay[k]);
+    }
+    // fixed-point exponent per instance
+    std::vector<int64_t> indeg(n, 0);
+    std::vector<float> maxw(n_inst, 0.0f);
+    for (int64_t k = 0; k < s; k++) {
+        indeg[dst[k]]++;
+        int g = inst ? inst[dst[k]] : 0;
+        maxw[g] = std::max(maxw[g], fabsf(weight[k]));
+    }
+    std::vector<int64_t> maxdeg(n_inst, 0);
+    for (int64_t i = 0; i < n; i++) {
+        int g = inst ? inst[i] : 0;
+        maxdeg[g] = std::max(maxdeg[g], indeg[i]);
+    }
+    std::vector<int32_t> qexp(n_inst);
+    for (int g = 0; g < n_inst; g++) qexp[g] = choose_qexp(maxdeg[g], maxw[g]);
+
+    Engine *e = new Engine();
+    int rc = init_device(*e, opt);
+    if (rc != BSIM_OK) { free_engine(e); return rc; }
+    e->N = n;
+    e->S = s;
+    e->D = D;
+    e->n_inst = n_inst;
+    e->n_pops = n_pops;
+    e->qexp = qexp;
+
+    // fold and deduplicate parameter classes
+    std::vector<float4> state(n);
+    std::vector<float> vtmp(n);
+    std::vector<uint16_t> cls(n);
+    std::vector<ClassParams> ctab;
+    std::map<std::vector<uint32_t>, int> cmap;
+    for (int64_t i = 0; i < n; i++) {
+        Folded f = fold_lif(params + 10 * i, dt);
+        int g = inst ? inst[i] : 0;
+        int pp = pop ? pop[i] : 0;
+        std::vector<uint32_t> key = {f2u(f.Cm), f2u(f.CE), f2u(f.CI), f2u(f.C_E), f2u(f.C_I), f2u(f.v_thresh),
+                                     f2u(f.v_reset), (uint32_t)f.refrac_time, (uint32_t)g, (uint32_t)pp};
+        auto it = cmap.find(key);
+        int c;
+        if (it == cmap.end()) {
+            if ((int)ctab.size() >= BSIM_MAX_CLASSES) {
+                free_engine(e);
+                return fail(BSIM_ERR_LIMIT, "bsim_create: more than 65535 distinct LIF parameter classes");
+            }
+            ClassParams cp;
+            cp.Cm = f.Cm; cp.CE = f.CE; cp.CI = f.CI; cp.C_E = f.C_E; cp.C_I = f.C_I;
+            cp.v_thresh = f.v_thresh; cp.v_reset = f.v_reset; cp.refrac_time = f.refrac_time;
+            cp.scale_up = ldexpf(1.0f, qexp[g]);
+            cp.scale_down = ldexpf(1.0f, -qexp[g]);
+            cp.pop = pp;
+            cp.inst = g;
+            c = (int)ctab.size();
+            ctab.push_back(cp);
+            cmap.emplace(key, c);
+        } else {
+            c = it->second;
+        }
+        cls[i] = (uint16_t)c;
+        vtmp[i] = f.v_tmp;
+        state[i] = make_float4(f.v_init, 0.0f, 0.0f, 0.0f);  // refrac_step = 0 (int bits 0)
+    }
+    e->n_cls = (int)ctab.size();
+
+    // push rows: counting sort by (source, delay), creation order kept inside a row
+    // (the order of BuildNetwork.cpp:96-136)
+    const int64_t nrows = n * (int64_t)D;
+    std::vector<int64_t> row_off(nrows + 1, 0);
+    for (int64_t k = 0; k < s; k++) row_off[(int64_t)src[k] * D + delay[k] - 1 + 1]++;
+    for (int64_t r = 0; r < nrows; r++) row_off[r + 1] += row_off[r];
+    std::vector<uint2> syn(s > 0 ? s : 1);
+    {
+        std::vector<int64_t> cur(row_off.begin(), row_off.end() - 1);
+        for (int64_t k = 0; k < s; k++) {
+            int64_t at = cur[(int64_t)src[k] * D + delay[k] - 1]++;
+            syn[at] = make_uint2((uint32_t)dst[k], f2u(weight[k]));
+        }
+    }
+    StepArgs &a = e->a;
+    a.N = n;
+    a.D = D;
+    float4 *d_state;
+    float *d_vtmp;
+    uint16_t *d_cls;
+    int64_t *d_row;
+    uint2 *d_syn;
+    if ((rc = dalloc(*e, &d_state, n)) || (rc = dalloc(*e, &d_vtmp, n)) || (rc = dalloc(*e, &d_cls, n)) ||
+        (rc = dalloc(*e, &d_row, nrows + 1)) || (rc = dalloc(*e, &d_syn, s))) {
+        free_engine(e);
+        return rc;
+    }
+    cudaMemcpy(d_state, state.data(), sizeof(float4) * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(d_vtmp, vtmp.data(), sizeof(float) * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(d_cls, cls.data(), sizeof(uint16_t) * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(d_row, row_off.data(), sizeof(int64_t) * (nrows + 1), cudaMemcpyHostToDevice);
+    if (s > 0) cudaMemcpy(d_syn, syn.data(), sizeof(uint2) * s, cudaMemcpyHostToDevice);
+    a.state = d_state;
+    a.vtmp = d_vtmp;
+    a.cls = d_cls;
+    a.row_off = d_row;
+    a.syn = d_syn;
+    std::vector<uint2>().swap(syn);
+
+    if (e->opt.build_pull) {
+        // pull rows: counting sort by target, creation order kept inside a row
+        std::vector<int64_t> col_off(n + 1, 0);
+        for (int64_t k = 0; k < s; k++) col_off[dst[k] + 1]++;
+        for (int64_t i = 0; i < n; i++) col_off[i + 1] += col_off[i];
+        std::vector<uint32_t> csrc(s > 0 ? s : 1);
+        std::vector<float> cw(s > 0 ? s : 1);
+        std::vector<uint8_t> cd(s > 0 ? s : 1);
+        if (D > 256) {
+            free_engine(e);
+            return fail(BSIM_ERR_LIMIT, "bsim_create: pull delivery supports delays up to 256 steps");
+        }
+        std::vector<int64_t> cur(col_off.begin(), col_off.end() - 1);
+        for (int64_t k = 0; k < s; k++) {
+            int64_t at = cur[dst[k]]++;
+            csrc[at] = (uint32_t)src[k];
+            cw[at] = weight[k];
+            cd[at] = (uint8_t)(delay[k] - 1);
+        }
+        int64_t *d_col;
+        uint32_t *d_csrc;
+        float *d_cw;
+        uint8_t *d_cd;
+        if ((rc = dalloc(*e, &d_col, n + 1)) || (rc = dalloc(*e, &d_csrc, s)) || (rc = dalloc(*e, &d_cw, s)) ||
+            (rc = dalloc(*e, &d_cd, s))) {
+            free_engine(e);
+            return rc;
+        }
+        cudaMemcpy(d_col, col_off.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice);
+        if (s > 0) {
+            cudaMemcpy(d_csrc, csrc.data(), sizeof(uint32_t) * s, cudaMemcpyHostToDevice);
+            cudaMemcpy(d_cw, cw.data(), sizeof(float) * s, cudaMemcpyHostToDevice);
+            cudaMemcpy(d_cd, cd.data(), s, cudaMemcpyHostToDevice);
+        }
+        a.col_off = d_col;
+        a.csc_src = d_csrc;
+        a.csc_w = d_cw;
+        a.csc_d = d_cd;
+    }
+    cudaError_t st = cudaGetLastError();
+    if (st != cudaSuccess) {
+        free_engine(e);
+        return fail(BSIM_ERR_CUDA, std::string("bsim_create upload: ") + cudaGetErrorString(st));
+    }
+    rc = finish_engine(*e, ctab);
+    if (rc != BSIM_OK) {
+        free_engine(e);
+        return rc;
+    }
+    *out = e;
+    return BSIM_OK;
+}
+
+// Ring, bitmaps, accumulators, counters; launch shape. Shared by both builders.
+static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
+{
+    StepArgs &a = e.a;
+    a.N = e.N;
+    a.D = e.D;
+    a.R = e.D + 2;
+    a.cap = e.N;
+    a.W = (e.N + 31) / 32;
+    ClassParams *d_ctab;
+    TRY(dalloc(e, &d_ctab, ctab.size()));
+    CK(cudaMemcpy(d_ctab, ctab.data(), sizeof(ClassParams) * ctab.size(), cudaMemcpyHostToDevice));
+    a.ctab = d_ctab;
+    size_t acc_elem = e.opt.accumulate == BSIM_ACC_ORDERED ? sizeof(float2) : sizeof(longlong2);
+    char *d_acc;
+    TRY(dalloc(e, &d_acc, acc_elem * 2 * (size_t)e.N));
+    CK(cudaMemset(d_acc, 0, acc_elem * 2 * (size_t)e.N));
+    a.acc = d_acc;
+    uint32_t *d_bm;
+    TRY(dalloc(e, &d_bm, (size_t)a.R * a.W));
+    CK(cudaMemset(d_bm, 0, sizeof(uint32_t) * (size_t)a.R * a.W));
+    a.bitmap = d_bm;
+    int32_t *d_ring, *d_ring_cnt, *d_fc, *d_err;
+    TRY(dalloc(e, &d_ring, (size_t)a.R * a.cap));
+    TRY(dalloc(e, &d_ring_cnt, a.R));
+    CK(cudaMemset(d_ring_cnt, 0, sizeof(int32_t) * a.R));
+    TRY(dalloc(e, &d_fc, e.N));
+    CK(cudaMemset(d_fc, 0, sizeof(int32_t) * e.N));
+    TRY(dalloc(e, &d_err, 1));
+    CK(cudaMemset(d_err, 0, sizeof(int32_t)));
+    a.ring = d_ring;
+    a.ring_cnt = d_ring_cnt;
+    a.fire_count = d_fc;
+    a.err = d_err;
+    unsigned long long *d_ctr;
+    TRY(dalloc(e, &d_ctr, 4));
+    CK(cudaMemset(d_ctr, 0, sizeof(unsigned long long) * 4));
+    a.step_ctr = d_ctr;
+    a.events = d_ctr + 1;
+    a.ticket = reinterpret_cast<unsigned int *>(d_ctr + 2);
+    a.delivery = e.opt.delivery == BSIM_DELIVERY_PULL ? BSIM_DELIVERY_PULL : BSIM_DELIVERY_PUSH;
+    a.deliv_sel = nullptr;
+    a.rec_ids = nullptr;
+    a.rec_off = nullptr;
+    a.rec = nullptr;
+    a.pop_hist = nullptr;
+    a.n_pops = e.n_pops;
+    a.hist_len = 0;
+    // launch shape: enough resident warps to cover HBM latency, at most one
+    // thread per neuron-group of work for small networks
+    e.block = e.opt.block_threads > 0 ? e.opt.block_threads : 512;
+    if (e.block % 32 != 0 || e.block > 512) return fail(BSIM_ERR_ARG, "block_threads must be a multiple of 32 <= 512");
+    int bps = 0;
+    CK(step_occupancy(e.block, e.opt.accumulate, &bps));
+    if (bps < 1) bps = 1;
+    e.grid = e.opt.grid_blocks > 0 ? e.opt.grid_blocks : e.sm_count * bps;
+    CK(cudaDeviceSynchronize());
+    return BSIM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Generated networks, built on the device.
+// ---------------------------------------------------------------------------
+#define GEN_MAX_DELAY 64
+#define GEN_MAX_IN 8  // incoming projections per population handled by the device builder
+
+struct GenInst {
+    int64_t nbase;       // first global neuron id
+    int32_t P, n, D;
+    int32_t cls_base;    // class id of population 0 (class = cls_base + pop)
+    uint64_t seed;
+    uint32_t p24, exc24;
+    float w_exc, w_inh;
+    int32_t proj_off;    // into the projection table
+    int32_t in_off;      // into the incoming table: [P][GEN_MAX_IN+1] (count, then projection ids)
+    int32_t out_off;     // into the outgoing table: [P][3] (count, projection ids)
+};
+
+struct GenProj {
+    int32_t src_pop, dst_pop;
+    uint64_t pseed;
+};
+
+struct GenDev {
+    const GenInst *inst;
+    int32_t n_inst;
+    const GenProj *proj;
+    const int32_t *in_tab;
+    const int32_t *out_tab;
+    int32_t D;  // engine max delay
+};
+
+static __device__ __forceinline__ int find_inst(const GenDev &g, int64_t gid)
+{
+    int lo = 0, hi = g.n_inst - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (g.inst[mid].nbase <= gid) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Per-neuron state, v_tmp and class id. rm and Cm come from the host fold of
+// each class so v_tmp = (i_offset*rm + v_rest) * (1 - Cm) rounds as on the host.
+__global__ void gen_neurons_kernel(GenDev g, const bsim_gen_spec *specs, const float *cls_rm, const float *cls_Cm,
+                                   float4 *state, float *vtmp, uint16_t *cls, int64_t N)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const int k = find_inst(g, i);
+        const GenInst &gi = g.inst[k];
+        const int64_t li = i - gi.nbase;
+        const int pop = (int)(li / gi.n);
+        const bsim_gen_spec &sp = specs[k];
+        float ioff, vinit;
+        draw_neuron(gi.seed, (uint64_t)li, sp, &ioff, &vinit);
+        const int c = gi.cls_base + pop;
+        const float rm = cls_rm[c], Cm = cls_Cm[c];
+        float vt = __fadd_rn(__fmul_rn(ioff, rm), sp.v_rest);
+        vt = __fmul_rn(vt, __fsub_rn(1.0f, Cm));
+        vtmp[i] = vt;
+        cls[i] = (uint16_t)c;
+        state[i] = make_float4(vinit, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+// Push rows: one warp per source neuron. Pass 0 counts entries per (source,
+// delay); pass 1 writes them in creation order (projection, then target).
+template <int PASS>
+__global__ void gen_push_kernel(GenDev g, int64_t N, int64_t *row_cnt_or_off, uint2 *syn)
+{
+    __shared__ long long s_cur[8][GEN_MAX_DELAY];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int D = g.D;
+    long long *cur = s_cur[wib];
+    for (int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < N;
+         s += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int k = find_inst(g, s);
+        const GenInst &gi = g.inst[k];
+        const int64_t ls = s - gi.nbase;
+        const int pop = (int)(ls / gi.n);
+        const int64_t i = ls - (int64_t)pop * gi.n;
+        for (int d = lane; d < D; d += 32) cur[d] = PASS == 0 ? 0 : row_cnt_or_off[s * D + d];
+        __syncwarp();
+        const int nout = g.out_tab[gi.out_off + 3 * pop];
+        for (int q = 0; q < nout; q++) {
+            const GenProj pr = g.proj[gi.proj_off + g.out_tab[gi.out_off + 3 * pop + 1 + q]];
+            const int64_t tbase = gi.nbase + (int64_t)pr.dst_pop * gi.n;
+            for (int j0 = 0; j0 < gi.n; j0 += 32) {
+                const int j = j0 + lane;
+                SynDraw sd;
+                bool conn = j < gi.n && draw_pair(pr.pseed, (uint64_t)i, (uint64_t)j, gi.p24, gi.exc24, gi.w_exc,
+                                                  gi.w_inh, gi.D, &sd);
+                const unsigned m = __ballot_sync(0xffffffffu, conn);
+                if (!m) continue;
+                const unsigned same = __match_any_sync(0xffffffffu, conn ? sd.d : -1);
+                if (conn) {
+                    const int leader = __ffs(same) - 1;
+                    const int rank = __popc(same & ((1u << lane) - 1u));
+                    const long long at = cur[sd.d - 1] + rank;
+                    if (PASS == 1) syn[at] = make_uint2((uint32_t)(tbase + j), __float_as_uint(sd.w));
+                    __syncwarp(same);
+                    if (lane == leader) cur[sd.d - 1] += __popc(same);
+                }
+                __syncwarp();
+            }
+        }
+        __syncwarp();
+        if (PASS == 0)
+            for (int d = lane; d < D; d += 32) row_cnt_or_off[s * D + d] = cur[d];
+        __syncwarp();
+    }
+}
+
+// Pull rows: one warp per target neuron over its incoming projections in
+// creation order, sources ascending inside a projection. Pass 0 counts and
+// reduces the per-instance max in-degree and max |w|; pass 1 writes.
+template <int PASS>
+__global__ void gen_pull_kernel(GenDev g, int64_t N, int64_t *col_cnt_or_off, uint32_t *csrc, float *cw,
+                                uint8_t *cd, unsigned long long *inst_maxdeg, unsigned int *inst_maxw)
+{
+    const int lane = threadIdx.x & 31;
+    for (int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < N;
+         t += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int k = find_inst(g, t);
+        const GenInst &gi = g.inst[k];
+        const int64_t lt = t - gi.nbase;
+        const int pop = (int)(lt / gi.n);
+        const int64_t j = lt - (int64_t)pop * gi.n;
+        long long at = PASS == 0 ? 0 : col_cnt_or_off[t];
+        float mw = 0.0f;
+        const int nin = g.in_tab[gi.in_off + (GEN_MAX_IN + 1) * pop];
+        for (int q = 0; q < nin; q++) {
+            const GenProj pr = g.proj[gi.proj_off + g.in_tab[gi.in_off + (GEN_MAX_IN + 1) * pop + 1 + q]];
+            const int64_t sbase = gi.nbase + (int64_t)pr.src_pop * gi.n;
+            for (int i0 = 0; i0 < gi.n; i0 += 32) {
+                const int i = i0 + lane;
+                SynDraw sd;
+                bool conn = i < gi.n && draw_pair(pr.pseed, (uint64_t)i, (uint64_t)j, gi.p24, gi.exc24, gi.w_exc,
+                                                  gi.w_inh, gi.D, &sd);
+                const unsigned m = __ballot_sync(0xffffffffu, conn);
+                if (conn) {
+                    const long long pos = at + __popc(m & ((1u << lane) - 1u));
+                    if (PASS == 1) {
+                        csrc[pos] = (uint32_t)(sbase + i);
+                        cw[pos] = sd.w;
+                        cd[pos] = (uint8_t)(sd.d - 1);
+                    } else {
+                        mw = fmaxf(mw, fabsf(sd.w));
+                    }
+                }
+                at += __popc(m);
+            }
+        }
+        if (PASS == 0) {
+            for (int o = 16; o > 0; o >>= 1) mw = fmaxf(mw, __shfl_xor_sync(0xffffffffu, mw, o));
+            if (lane == 0) {
+                col_cnt_or_off[t] = at;
+                atomicMax(&inst_maxdeg[k], (unsigned long long)at);
+                atomicMax(&inst_maxw[k], __float_as_uint(mw));
+            }
+        }
+    }
+}
+
+// Remote projection choice of one generated network (host side, shared by
+// the host generator and the device builder).
+struct GenPlan {
+    std::vector<GenProj> proj;              // creation order
+    std::vector<std::vector<int>> in, out;  // per population: projection ids in creation order
+};
+
+static GenPlan gen_plan(const bsim_gen_spec &g)
+{
+    GenPlan pl;
+    const int P = g.n_pop;
+    pl.in.assign(P, {});
+    pl.out.assign(P, {});
+    for (int k = 0; k + 1 < P; k++) pl.proj.push_back({k, k + 1, proj_seed(g.seed, k)});
+    if (P >= 2) {
+        int m = (int)(g.remote_frac * (float)P + 0.5f);
+        m = std::min(m, P);
+        std::vector<std::pair<uint64_t, int>> keys;
+        for (int k = 0; k < P; k++) keys.push_back({hash3(g.seed ^ SALT_REMOTE_SEL, (uint64_t)k, 0), k});
+        std::sort(keys.begin(), keys.end());
+        std::vector<int> sel;
+        for (int r = 0; r < m; r++) sel.push_back(keys[r].second);
+        std::sort(sel.begin(), sel.end());
+        for (int k : sel) {
+            uint64_t h = hash3(g.seed ^ SALT_REMOTE_TGT, (uint64_t)k, 0);
+            int tgt = (int)((k + 1 + (int64_t)(h % (uint64_t)(P - 1))) % P);
+            int id = (int)pl.proj.size();
+            pl.proj.push_back({k, tgt, proj_seed(g.seed, id)});
+        }
+    }
+    for (int id = 0; id < (int)pl.proj.size(); id++) {
+        pl.out[pl.proj[id].src_pop].push_back(id);
+        pl.in[pl.proj[id].dst_pop].push_back(id);
+    }
+    return pl;
+}
+
+static int check_spec(const bsim_gen_spec &g)
+{
+    if (g.n_pop < 1 || g.pop_size < 1 || g.max_delay < 1 || g.max_delay > GEN_MAX_DELAY ||
+        (int64_t)g.n_pop * g.pop_size > (int64_t)INT32_MAX / 2 || !(g.p_conn >= 0) || g.p_conn > 1)
+        return fail(BSIM_ERR_ARG, "bsim_gen_spec: invalid sizes (max_delay 1..64, p_conn in [0,1])");
+    return BSIM_OK;
+}
+
+static void spec_params(const bsim_gen_spec &g, float ioff, float vinit, float *p)
+{
+    p[0] = vinit; p[1] = g.v_rest; p[2] = g.v_reset; p[3] = g.cm; p[4] = g.tau_m;
+    p[5] = g.tau_refrac; p[6] = g.tau_syn_E; p[7] = g.tau_syn_I; p[8] = g.v_thresh; p[9] = ioff;
+}
+
+static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, const bsim_options *opt, Engine **out)
+{
+    if (!specs || ns < 1 || !(dt > 0) || !out) return fail(BSIM_ERR_ARG, "bsim_create_generated: invalid arguments");
+    std::vector<GenInst> gi(ns);
+    std::vector<GenProj> proj;
+    std::vector<int32_t> in_tab, out_tab;
+    int64_t N = 0;
+    int32_t D = 1, n_cls = 0;
+    std::vector<ClassParams> ctab;
+    std::vector<float> cls_rm, cls_Cm;
+    for (int k = 0; k < ns; k++) {
+        const bsim_gen_spec &g = specs[k];
+        TRY(check_spec(g));
+        GenPlan pl = gen_plan(g);
+        GenInst &x = gi[k];
+        x.nbase = N;
+        x.P = g.n_pop;
+        x.n = g.pop_size;
+        x.D = g.max_delay;
+        x.cls_base = n_cls;
+        x.seed = g.seed;
+        x.p24 = prob24(g.p_conn);
+        x.exc24 = prob24(g.exc_frac);
+        x.w_exc = g.w_max;
+        x.w_inh = g.inh_scale * g.w_max;
+        x.proj_off = (int32_t)proj.size();
+        x.in_off = (int32_t)in_tab.size();
+        x.out_off = (int32_t)out_tab.size();
+        for (auto &p : pl.proj) proj.push_back(p);
+        for (int p = 0; p < g.n_pop; p++) {
+            if ((int)pl.in[p].size() > GEN_MAX_IN) return fail(BSIM_ERR_LIMIT, "generator: too many incoming projections");
+            in_tab.push_back((int32_t)pl.in[p].size());
+            for (int q = 0; q < GEN_MAX_IN; q++) in_tab.push_back(q < (int)pl.in[p].size() ? pl.in[p][q] : -1);
+            out_tab.push_back((int32_t)pl.out[p].size());
+            for (int q = 0; q < 2; q++) out_tab.push_back(q < (int)pl.out[p].size() ? pl.out[p][q] : -1);
+        }
+        N += (int64_t)g.n_pop * g.pop_size;
+        D = std::max(D, g.max_delay);
+        // one class per population; i_offset / v_init only change v_tmp and the initial state
+        float prm[10];
+        spec_params(g, 0.0f, 0.0f, prm);
+        Folded f = fold_lif(prm, dt);
+        const float ZERO = 1e-10f;
+        float rm = fabsf(g.cm) > ZERO ? g.tau_m / g.cm : 1.0f;
+        for (int p = 0; p < g.n_pop; p++) {
+            ClassParams cp;
+            cp.Cm = f.Cm; cp.CE = f.CE; cp.CI = f.CI; cp.C_E = f.C_E; cp.C_I = f.C_I;
+            cp.v_thresh = f.v_thresh; cp.v_reset = f.v_reset; cp.refrac_time = f.refrac_time;
+            cp.pop = n_cls + p;
+            cp.inst = k;
+            ctab.push_back(cp);
+            cls_rm.push_back(rm);
+            cls_Cm.push_back(f.Cm);
+        }
+        n_cls += g.n_pop;
+        if (n_cls > BSIM_MAX_CLASSES) return fail(BSIM_ERR_LIMIT, "generator: more than 65535 populations");
+    }
+    if (N > (int64_t)INT32_MAX - 64) return fail(BSIM_ERR_LIMIT, "generator: more than 2^31-64 neurons");
+
+    Engine *e = new Engine();
+    int rc = init_device(*e, opt);
+    if (rc != BSIM_OK) { free_engine(e); return rc; }
+    e->N = N;
+    e->D = D;
+    e->n_inst = ns;
+    e->n_cls = n_cls;
+    e->n_pops = n_cls;
+    Engine &E = *e;
+    auto bail = [&](int r) { free_engine(e); return r; };
+
+    // small tables (freed at the end of the build)
+    std::vector<void *> tmp;
+    auto talloc = [&](void **p, size_t bytes) -> int {
+        cudaError_t st = cudaMalloc(p, bytes ? bytes : 1);
+        if (st != cudaSuccess) { cudaGetLastError(); return fail(BSIM_ERR_NOMEM, "build scratch allocation failed"); }
+        tmp.push_back(*p);
+        return BSIM_OK;
+    };
+    auto free_tmp = [&]() { for (void *p : tmp) cudaFree(p); tmp.clear(); };
+    GenInst *d_gi; GenProj *d_proj; int32_t *d_in, *d_out; bsim_gen_spec *d_specs; float *d_rm, *d_Cm;
+    if ((rc = talloc((void **)&d_gi, sizeof(GenInst) * ns)) || (rc = talloc((void **)&d_proj, sizeof(GenProj) * std::max<size_t>(1, proj.size()))) ||
+        (rc = talloc((void **)&d_in, sizeof(int32_t) * in_tab.size())) || (rc = talloc((void **)&d_out, sizeof(int32_t) * out_tab.size())) ||
+        (rc = talloc((void **)&d_specs, sizeof(bsim_gen_spec) * ns)) || (rc = talloc((void **)&d_rm, sizeof(float) * n_cls)) ||
+        (rc = talloc((void **)&d_Cm, sizeof(float) * n_cls))) { free_tmp(); return bail(rc); }
+    cudaMemcpy(d_gi, gi.data(), sizeof(GenInst) * ns, cudaMemcpyHostToDevice);
+    if (!proj.empty()) cudaMemcpy(d_proj, proj.data(), sizeof(GenProj) * proj.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_in, in_tab.data(), sizeof(int32_t) * in_tab.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_out, out_tab.data(), sizeof(int32_t) * out_tab.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_specs, specs, sizeof(bsim_gen_spec) * ns, cudaMemcpyHostToDevice);
+    cudaMemcpy(d_rm, cls_rm.data(), sizeof(float) * n_cls, cudaMemcpyHostToDevice);
+    cudaMemcpy(d_Cm, cls_Cm.data(), sizeof(float) * n_cls, cudaMemcpyHostToDevice);
+    GenDev gd{d_gi, ns, d_proj, d_in, d_out, D};
+
+    float4 *d_state; float *d_vtmp; uint16_t *d_cls;
+    if ((rc = dalloc(E, &d_state, N)) || (rc = dalloc(E, &d_vtmp, N)) || (rc = dalloc(E, &d_cls, N))) { free_tmp(); return bail(rc); }
+    const int gb = E.sm_count * 8;
+    gen_neurons_kernel<<<gb, 256, 0, E.stream>>>(gd, d_specs, d_rm, d_Cm, d_state, d_vtmp, d_cls, N);
+
+    // in-degree and max |w| per instance -> fixed-point exponents
+    int64_t *d_col;
+    unsigned long long *d_maxdeg; unsigned int *d_maxw;
+    if ((rc = dalloc(E, &d_col, N + 1)) || (rc = talloc((void **)&d_maxdeg, 8 * ns)) || (rc = talloc((void **)&d_maxw, 4 * ns))) { free_tmp(); return bail(rc); }
+    cudaMemsetAsync(d_maxdeg, 0, 8 * ns, E.stream);
+    cudaMemsetAsync(d_maxw, 0, 4 * ns, E.stream);
+    cudaMemsetAsync(d_col + N, 0, 8, E.stream);
+    gen_pull_kernel<0><<<gb, 256, 0, E.stream>>>(gd, N, d_col, nullptr, nullptr, nullptr, d_maxdeg, d_maxw);
+    // exclusive scan of the counts (in place via a temp copy) -> col_off
+    auto scan = [&](int64_t *arr, int64_t count) -> int {
+        int64_t *d_tmp;
+        if (talloc((void **)&d_tmp, sizeof(int64_t) * (count + 1))) return BSIM_ERR_NOMEM;
+        cudaMemcpyAsync(d_tmp, arr, sizeof(int64_t) * count, cudaMemcpyDeviceToDevice, E.stream);
+        cudaMemsetAsync(d_tmp + count, 0, 8, E.stream);
+        size_t tb = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, tb, d_tmp, arr, count + 1, E.stream);
+        void *d_tb;
+        if (talloc(&d_tb, tb)) return BSIM_ERR_NOMEM;
+        cub::DeviceScan::ExclusiveSum(d_tb, tb, d_tmp, arr, count + 1, E.stream);
+        return BSIM_OK;
+    };
+    if ((rc = scan(d_col, N))) { free_tmp(); return bail(rc); }
+    int64_t S = 0;
+    std::vector<unsigned long long> maxdeg(ns);
+    std::vector<unsigned int> maxw(ns);
+    cudaMemcpyAsync(&S, d_col + N, 8, cudaMemcpyDeviceToHost, E.stream);
+    cudaMemcpyAsync(maxdeg.data(), d_maxdeg, 8 * ns, cudaMemcpyDeviceToHost, E.stream);
+    cudaMemcpyAsync(maxw.data(), d_maxw, 4 * ns, cudaMemcpyDeviceToHost, E.stream);
+    if (cudaStreamSynchronize(E.stream) != cudaSuccess) { free_tmp(); return bail(fail(BSIM_ERR_CUDA, std::string("generator: ") + cudaGetErrorString(cudaGetLastError()))); }
+    E.S = S;
+    E.qexp.resize(ns);
+    for (int k = 0; k < ns; k++) {
+        float mw;
+        memcpy(&mw, &maxw[k], 4);
+        E.qexp[k] = choose_qexp((int64_t)maxdeg[k], mw);
+    }
+    for (auto &cp : ctab) {
+        cp.scale_up = ldexpf(1.0f, E.qexp[cp.inst]);
+        cp.scale_down = ldexpf(1.0f, -E.qexp[cp.inst]);
+    }
+    if (E.opt.build_pull) {
+        uint32_t *d_csrc; float *d_cw; uint8_t *d_cd;
+        if ((rc = dalloc(E, &d_csrc, S)) || (rc = dalloc(E, &d_cw, S)) || (rc = dalloc(E, &d_cd, S))) { free_tmp(); return bail(rc); }
+        gen_pull_kernel<1><<<gb, 256, 0, E.stream>>>(gd, N, d_col, d_csrc, d_cw, d_cd, nullptr, nullptr);
+        E.a.col_off = d_col;
+        E.a.csc_src = d_csrc;
+        E.a.csc_w = d_cw;
+        E.a.csc_d = d_cd;
+    }
+    // push rows
+    const int64_t nrows = N * (int64_t)D;
+    int64_t *d_row; uint2 *d_syn;
+    if ((rc = dalloc(E, &d_row, nrows + 1)) || (rc = dalloc(E, &d_syn, S))) { free_tmp(); return bail(rc); }
+    gen_push_kernel<0><<<gb, 256, 0, E.stream>>>(gd, N, d_row, nullptr);
+    if ((rc = scan(d_row, nrows))) { free_tmp(); return bail(rc); }
+    gen_push_kernel<1><<<gb, 256, 0, E.stream>>>(gd, N, d_row, d_syn);
+    cudaError_t st = cudaStreamSynchronize(E.stream);
+    if (st == cudaSuccess) st = cudaGetLastError();
+    free_tmp();
+    if (st != cudaSuccess) return bail(fail(BSIM_ERR_CUDA, std::string("generator kernels: ") + cudaGetErrorString(st)));
+    E.a.state = d_state;
+    E.a.vtmp = d_vtmp;
+    E.a.cls = d_cls;
+    E.a.row_off = d_row;
+    E.a.syn = d_syn;
+    rc = finish_engine(E, ctab);
+    if (rc != BSIM_OK) return bail(rc);
+    *out = e;
+    return BSIM_OK;
+}
+
+// Host generator: the same draws, emitted in global creation order.
+static int gen_host(const bsim_gen_spec &g, float *params, int32_t *pop, int32_t *src, int32_t *dst, float *w,
+                    int32_t *d, int64_t *n_out, int64_t *s_out)
+{
+    TRY(check_spec(g));
+    GenPlan pl = gen_plan(g);
+    const int64_t n = (int64_t)g.n_pop * g.pop_size;
+    if (params || pop) {
+        for (int64_t i = 0; i < n; i++) {
+            float ioff, vinit;
+            draw_neuron(g.seed, (uint64_t)i, g, &ioff, &vinit);
+            if (params) spec_params(g, ioff, vinit, params + 10 * i);
+            if (pop) pop[i] = (int32_t)(i / g.pop_size);
+        }
+    }
+    const uint32_t p24 = prob24(g.p_conn), exc24 = prob24(g.exc_frac);
+    const float w_exc = g.w_max, w_inh = g.inh_scale * g.w_max;
+    int64_t s = 0;
+    for (const GenProj &pr : pl.proj) {
+        for (int64_t i = 0; i < g.pop_size; i++) {
+            for (int64_t j = 0; j < g.pop_size; j++) {
+                SynDraw sd;
+                if (!draw_pair(pr.pseed, (uint64_t)i, (uint64_t)j, p24, exc24, w_exc, w_inh, g.max_delay, &sd)) continue;
+                if (src) {
+                    src[s] = (int32_t)(pr.src_pop * (int64_t)g.pop_size + i);
+                    dst[s] = (int32_t)(pr.dst_pop * (int64_t)g.pop_size + j);
+                    w[s] = sd.w;
+                    d[s] = sd.d;
+                }
+                s++;
+            }
+        }
+    }
+    if (n_out) *n_out = n;
+    if (s_out) *s_out = s;
+    return BSIM_OK;
+}
+
+}  // namespace bsim
+
+using namespace bsim;
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+// The C handle is the engine itself behind an opaque pointer type.
+static Engine *H(bsim_engine *h) { return reinterpret_cast<Engine *>(h); }
+static bsim_engine *Hc(Engine *e) { return reinterpret_cast<bsim_engine *>(e); }
+
+extern "C" {
+
+int bsim_options_default(bsim_options *opt)
+{
+    if (!opt) return fail(BSIM_ERR_ARG, "null options");
+    memset(opt, 0, sizeof(*opt));
+    opt->device = 0;
+    opt->accumulate = BSIM_ACC_EXACT;
+    opt->delivery = BSIM_DELIVERY_PUSH;
+    opt->build_pull = 0;
+    opt->graph_steps = 64;
+    return BSIM_OK;
+}
+
+int bsim_create(const float *params, int64_t n, const int32_t *pop, const int32_t *instance, const int32_t *src,
+                const int32_t *dst, const float *weight, const int32_t *delay_steps, int64_t s, float dt,
+                const bsim_options *opt, bsim_engine **out)
+{
+    Engine *e = nullptr;
+    int rc = create_from_arrays(params, n, pop, instance, src, dst, weight, delay_steps, s, dt, opt, &e);
+    if (rc == BSIM_OK) *out = Hc(e);
+    return rc;
+}
+
+int bsim_create_generated(const bsim_gen_spec *specs, int32_t n_specs, float dt, const bsim_options *opt,
+                          bsim_engine **out)
+{
+    Engine *e = nullptr;
+    int rc = create_generated(specs, n_specs, dt, opt, &e);
+    if (rc == BSIM_OK) *out = Hc(e);
+    return rc;
+}
+
+int bsim_gen_count(const bsim_gen_spec *spec, int64_t *n, int64_t *s)
+{
+    if (!spec) return fail(BSIM_ERR_ARG, "null spec");
+    return gen_host(*spec, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, n, s);
+}
+
+int bsim_gen_host(const bsim_gen_spec *spec, float *params, int32_t *pop, int32_t *src, int32_t *dst, float *weight,
+                  int32_t *delay_steps)
+{
+    if (!spec || !src || !dst || !weight || !delay_steps) return fail(BSIM_ERR_ARG, "null argument");
+    return gen_host(*spec, params, pop, src, dst, weight, delay_steps, nullptr, nullptr);
+}
+
+int bsim_synapse_reset(const float *delay_s, const float *weight, const float *tau_syn, int64_t s, float dt,
+                       int32_t *delay_steps, float *weight_out)
+{
+    if (s < 0 || (s > 0 && (!delay_s || !weight || !tau_syn || !delay_steps || !weight_out)))
+        return fail(BSIM_ERR_ARG, "bsim_synapse_reset: invalid arguments");
+    const float ZERO = 1e-10f;
+    for (int64_t i = 0; i < s; i++) {
+        int32_t st = (int32_t)roundf(delay_s[i] / dt);
+        float rem = delay_s[i] - dt * (float)st;
+        float w = weight[i];
+        if (fabsf(tau_syn[i]) > ZERO && fabsf(rem) > ZERO) w = w * expf(-rem / tau_syn[i]);
+        delay_steps[i] = st;
+        weight_out[i] = w;
+    }
+    return BSIM_OK;
+}
+
+static int check_err(Engine &e)
+{
+    int32_t err = 0;
+    CK(cudaMemcpy(&err, e.a.err, 4, cudaMemcpyDeviceToHost));
+    if (err) return fail(BSIM_ERR_DEVICE, "device error flag " + std::to_string(err));
+    return BSIM_OK;
+}
+
+int bsim_run_async(bsim_engine *eh, int64_t steps)
+{
+    if (!eh || steps < 0) return fail(BSIM_ERR_ARG, "bsim_run: invalid arguments");
+    Engine &e = *H(eh);
+    CK(cudaSetDevice(e.device));
+    int64_t left = steps;
+    const int gl = e.opt.graph_steps;
+    if (gl > 0 && left >= gl) {
+        if (!e.graph_exec || e.graph_len != gl) {
+            if (e.graph_exec) cudaGraphExecDestroy(e.graph_exec);
+            if (e.graph) cudaGraphDestroy(e.graph);
+            e.graph_exec = nullptr;
+            e.graph = nullptr;
+            CK(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
+            for (int i = 0; i < gl; i++) {
+                cudaError_t st = launch_step(e);
+                if (st != cudaSuccess) {
+                    cudaGraph_t g;
+                    cudaStreamEndCapture(e.stream, &g);
+                    if (g) cudaGraphDestroy(g);
+                    return fail(BSIM_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(st));
+                }
+            }
+            CK(cudaStreamEndCapture(e.stream, &e.graph));
+            CK(cudaGraphInstantiate(&e.graph_exec, e.graph, 0));
+            e.graph_len = gl;
+        }
+        while (left >= gl) {
+            CK(cudaGraphLaunch(e.graph_exec, e.stream));
+            left -= gl;
+        }
+    }
+    for (; left > 0; left--) CK(launch_step(e));
+    e.steps_done += steps;
+    return BSIM_OK;
+}
+
+int bsim_sync(bsim_engine *eh)
+{
+    if (!eh) return fail(BSIM_ERR_ARG, "null engine");
+    CK(cudaSetDevice(H(eh)->device));
+    CK(cudaStreamSynchronize(H(eh)->stream));
+    return check_err(*H(eh));
+}
+
+int bsim_run(bsim_engine *eh, int64_t steps)
+{
+    int rc = bsim_run_async(eh, steps);
+    if (rc != BSIM_OK) return rc;
+    return bsim_sync(eh);
+}
+
+int bsim_record(bsim_engine *eh, int64_t max_steps, int64_t capacity)
+{
+    if (!eh || max_steps < 0 || capacity < 0) return fail(BSIM_ERR_ARG, "bsim_record: invalid arguments");
+    Engine &e = *H(eh);
+    CK(cudaSetDevice(e.device));
+    CK(cudaStreamSynchronize(e.stream));
+    if (!e.a.rec) {
+        RecCtl *rc;
+        TRY(dalloc(e, &rc, 1));
+        e.a.rec = rc;
+        e.rec_dirty = true;
+    }
+    if (max_steps > e.rec_steps_alloc || capacity > e.rec_cap_alloc || !e.a.rec_ids) {
+        // grow the buffers; the captured graph holds the old pointers
+        int32_t *ids;
+        int64_t *off;
+        TRY(dalloc(e, &ids, std::max<int64_t>(capacity, e.rec_cap_alloc)));
+        TRY(dalloc(e, &off, std::max<int64_t>(max_steps, e.rec_steps_alloc) + 1));
+        e.a.rec_ids = ids;
+        e.a.rec_off = off;
+        e.rec_cap_alloc = std::max<int64_t>(capacity, e.rec_cap_alloc);
+        e.rec_steps_alloc = std::max<int64_t>(max_steps, e.rec_steps_alloc);
+        e.rec_dirty = true;
+    }
+    RecCtl ctl{e.steps_done, e.steps_done, max_steps, capacity};
+    CK(cudaMemset(e.a.rec_off, 0, sizeof(int64_t)));
+    CK(cudaMemcpy(e.a.rec, &ctl, sizeof(ctl), cudaMemcpyHostToDevice));
+    if (e.rec_dirty) {
+        if (e.graph_exec) { cudaGraphExecDestroy(e.graph_exec); e.graph_exec = nullptr; }
+        if (e.graph) { cudaGraphDestroy(e.graph); e.graph = nullptr; }
+        e.rec_dirty = false;
+    }
+    return BSIM_OK;
+}
+
+int bsim_read_raster(bsim_engine *eh, int64_t *step_off, int32_t *ids, int64_t ids_cap, int64_t *n_steps)
+{
+    if (!eh || !step_off || !n_steps) return fail(BSIM_ERR_ARG, "bsim_read_raster: invalid arguments");
+    Engine &e = *H(eh);
+    if (!e.a.rec || !e.a.rec_ids) return fail(BSIM_ERR_STATE, "bsim_read_raster: recording not enabled");
+    CK(cudaSetDevice(e.device));
+    CK(launch_record_flush(e));
+    CK(cudaStreamSynchronize(e.stream));
+    RecCtl ctl;
+    CK(cudaMemcpy(&ctl, e.a.rec, sizeof(ctl), cudaMemcpyDeviceToHost));
+    int64_t ns = ctl.next - ctl.t0;
+    if (ns < 0) ns = 0;
+    if (ns > ctl.steps) ns = ctl.steps;
+    CK(cudaMemcpy(step_off, e.a.rec_off, sizeof(int64_t) * (ns + 1), cudaMemcpyDeviceToHost));
+    *n_steps = ns;
+    int64_t total = step_off[ns];
+    if (total > ctl.cap) return fail(BSIM_ERR_LIMIT, "raster buffer overflowed");
+    if (ids) {
+        if (total > ids_cap) return fail(BSIM_ERR_ARG, "bsim_read_raster: ids buffer too small");
+        CK(cudaMemcpy(ids, e.a.rec_ids, sizeof(int32_t) * total, cudaMemcpyDeviceToHost));
+        for (int64_t k = 0; k < ns; k++) std::sort(ids + step_off[k], ids + step_off[k + 1]);
+    }
+    return BSIM_OK;
+}
+
+int bsim_read_state(bsim_engine *eh, float *v, float *iE, float *iI, int32_t *refrac)
+{
+    if (!eh) return fail(BSIM_ERR_ARG, "null engine");
+    Engine &e = *H(eh);
+    CK(cudaSetDevice(e.device));
+    CK(cudaStreamSynchronize(e.stream));
+    std::vector<float4> st(e.N);
+    CK(cudaMemcpy(st.data(), e.a.state, sizeof(float4) * e.N, cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < e.N; i++) {
+        if (v) v[i] = st[i].x;
+        if (iE) iE[i] = st[i].y;
+        if (iI) iI[i] = st[i].z;
+        if (refrac) memcpy(&refrac[i], &st[i].w, 4);
+    }
+    return BSIM_OK;
+}
+
+int bsim_write_state(bsim_engine *eh, const float *v, const float *iE, const float *iI, const int32_t *refrac)
+{
+    if (!eh) return fail(BSIM_ERR_ARG, "null engine");
+    Engine &e = *H(eh);
+    CK(cudaSetDevice(e.device));
+    CK(cudaStreamSynchronize(e.stream));
+    std::vector<float4> st(e.N);
+    if (!(v && iE && iI && refrac))  // partial update: keep the other fields
+        CK(cudaMemcpy(st.data(), e.a.state, sizeof(float4) * e.N, cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < e.N; i++) {
+        if (v) st[i].x = v[i];
+        if (iE) st[i].y = iE[i];
+        if (iI) st[i].z = iI[i];
+        if (refrac) memcpy(&st[i].w, &refrac[i], 4);
+    }
+    CK(cudaMemcpy(e.a.state, st.data(), sizeof(float4) * e.N, cudaMemcpyHostToDevice));
+    return BSIM_OK;
+}
+
+int bsim_get_stream(bsim_engine *eh, void **stream)
+{
+    if (!eh || !stream) return fail(BSIM_ERR_ARG, "invalid arguments");
+    *stream = (void *)H(eh)->stream;
+    return BSIM_OK;
+}
+
+int bsim_read_fire_count(bsim_engine *eh, int32_t *count)
+{
+    if (!eh || !count) return fail(BSIM_ERR_ARG, "invalid arguments");
+    Engine &e = *H(eh);
+    CK(cudaSetDevice(e.device));
+    CK(cudaStreamSynchronize(e.stream));
+    CK(cudaMemcpy(count, e.a.fire_count, sizeof(int32_t) * e.N, cudaMemcpyDeviceToHost));
+    return BSIM_OK;
+}
+
+int bsim_read_pop_counts(bsim_engine *eh, int32_t *counts, int32_t steps)
+{
+    (void)counts;
+    (void)steps;
+    if (!eh) return fail(BSIM_ERR_ARG, "null engine");
+    return fail(BSIM_ERR_STATE, "population statistics are not enabled on this engine");
+}
+
+int bsim_get_info(bsim_engine *eh, bsim_info *info)
+{
+    if (!eh || !info) return fail(BSIM_ERR_ARG, "invalid arguments");
+    Engine &e = *H(eh);
+    CK(cudaSetDevice(e.device));
+    CK(cudaStreamSynchronize(e.stream));
+    memset(info, 0, sizeof(*info));
+    info->n_neurons = e.N;
+    info->n_synapses = e.S;
+    info->max_delay = e.D;
+    info->n_instances = e.n_inst;
+    info->n_classes = e.n_cls;
+    info->n_pops = e.n_pops;
+    unsigned long long ctr[2];
+    CK(cudaMemcpy(ctr, e.a.step_ctr, sizeof(ctr), cudaMemcpyDeviceToHost));
+    info->steps_done = (int64_t)ctr[0];
+    info->events_total = ctr[1];
+    info->device_bytes = e.device_bytes;
+    info->grid_blocks = e.grid;
+    info->block_threads = e.block;
+    info->accumulate = e.opt.accumulate;
+    info->delivery = e.opt.delivery;
+    info->sm_count = e.sm_count;
+    return BSIM_OK;
+}
+
+int bsim_get_qexp(bsim_engine *eh, int32_t *qexp)
+{
+    if (!eh || !qexp) return fail(BSIM_ERR_ARG, "invalid arguments");
+    for (int i = 0; i < H(eh)->n_inst; i++) qexp[i] = H(eh)->qexp[i];
+    return BSIM_OK;
+}
+
+int bsim_destroy(bsim_engine *eh)
+{
+    if (!eh) return BSIM_OK;
+    free_engine(H(eh));
+    return BSIM_OK;
+}
+
+const char *bsim_last_error(void) { return g_err.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,93 @@
+// Internal structures of the bsim_b200 engine (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/bsim_b200.h"
+
+namespace bsim {
+
+// One folded LIF parameter tuple: the per-population part of LIFENeuron::reset's
+// output (src/neuron/lif/LIFENeuron.cpp:68-112). v_tmp depends on i_offset and is
+// kept per neuron. 48 bytes; the table is small and read through the L1 cache.
+struct ClassParams {
+    float Cm, CE, CI, C_E, C_I, v_thresh, v_reset;
+    int32_t refrac_time;
+    float scale_up;    // 2^qexp: fixed-point value of a weight is rn(w * scale_up)
+    float scale_down;  // 2^-qexp
+    int32_t pop;       // population (spike statistics)
+    int32_t inst;      // independent network
+};
+
+// Raster recording window: cycles [t0, t0 + steps) into a buffer of cap ids.
+struct RecCtl {
+    long long next;   // next cycle to copy out (cycle t copies cycle t-1 once it is complete)
+    long long t0;
+    long long steps;  // 0: not recording
+    long long cap;
+};
+
+// Everything one fused step launch needs. Passed by value (kernel parameter space).
+struct StepArgs {
+    int64_t N;         // neurons
+    int32_t D;         // max delay, steps
+    int32_t R;         // ring slots = D + 2
+    int64_t cap;       // fired ids per ring slot
+    int64_t W;         // bitmap words per ring slot = ceil(N / 32)
+    float4 *state;     // [N] {v, i_E, i_I, refrac_step as int bits}
+    const float *vtmp; // [N]
+    const uint16_t *cls;       // [N] class of each neuron
+    const ClassParams *ctab;   // [n_cls]
+    void *acc;                 // [2][N] longlong2 (EXACT) or float2 (ORDERED): input for the next step
+    uint32_t *bitmap;          // [R][W] fired flags of each step in the ring
+    int32_t *ring;             // [R][cap] fired ids of each step in the ring
+    int32_t *ring_cnt;         // [R]
+    const int64_t *row_off;    // [N*D + 1] push rows by (source, delay)
+    const uint2 *syn;          // [S] {target id, weight bits}, creation order inside a row
+    const int64_t *col_off;    // [N + 1] pull rows by target
+    const uint32_t *csc_src;   // [S] source id, creation order inside a row
+    const float *csc_w;        // [S]
+    const uint8_t *csc_d;      // [S] delay - 1
+    int32_t *fire_count;       // [N]
+    unsigned long long *step_ctr;  // current cycle t (device-side, advanced by the last block)
+    unsigned int *ticket;          // end-of-step block counter
+    unsigned long long *events;    // synaptic events delivered
+    int32_t *err;                  // device error flag (0 = ok)
+    const int32_t *deliv_sel;      // per-step delivery choice written by the predictor (may be NULL)
+    int32_t delivery;              // BSIM_DELIVERY_PUSH / _PULL when deliv_sel is NULL
+    // raster recording (control words in device memory so a captured graph stays valid)
+    int32_t *rec_ids;           // [rec->cap]
+    int64_t *rec_off;           // [rec->steps + 1]
+    struct RecCtl *rec;         // NULL: recording never enabled
+    // per-population spike counts of the last hist_len steps (predictor input)
+    int32_t *pop_hist;          // [hist_len][n_pops]
+    int32_t n_pops, hist_len;
+};
+
+struct Engine {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bsim_options opt{};
+    int sm_count = 0;
+    int64_t N = 0, S = 0;
+    int32_t D = 1;
+    int32_t n_inst = 1, n_cls = 0, n_pops = 1;
+    std::vector<int32_t> qexp;  // per instance
+    int64_t steps_done = 0;
+    int64_t device_bytes = 0;
+    std::vector<void *> allocs;
+    StepArgs a{};
+    int grid = 0, block = 0;
+    // CUDA graph of graph_steps fused steps
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_len = 0;
+    // recording
+    int64_t rec_cap_alloc = 0, rec_steps_alloc = 0;
+    bool rec_dirty = false;
+};
+
+}  // namespace bsim

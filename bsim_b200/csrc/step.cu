@@ -1,0 +1,388 @@
+// The fused simulation step for sm_100a.
+//
+// One launch advances every network in the engine by one cycle. Its blocks
+// first run the LIF_brian update over a grid-stride share of the neurons
+// (reads the synaptic input summed during the previous launch, writes the new
+// state, appends fired ids to this cycle's ring slot with one atomic per warp
+// and stores the warp's ballot as a fired-bitmap word), then deliver the
+// spikes of cycles t-1 .. t-D into the input buffer of cycle t+1.
+//
+// The two halves touch disjoint data (the input accumulators are double
+// buffered by cycle parity, the fire ring has D+2 slots), so they need no
+// barrier between them; the kernel boundary orders consecutive cycles.
+// The cycle counter lives on the device and is advanced by the last block to
+// finish, so the same launch can be replayed from a CUDA graph with no host
+// involvement.
+//
+// Reference semantics (BSim, paths relative to its root):
+//   neuron update  LIFENeuron::update  src/neuron/lif/LIFENeuron.cpp:114-160
+//                  (GPU: find_life_neuron + update_life_neuron, src/neuron/lif/lif.cu:9-162)
+//   delivery       update_dense_static_hit, src/synapse/static/static.cu:59-96:
+//                  at cycle t, ring slot t-d feeds the synapses of delay d
+//   ring advance   update_time, src/gpu_utils/runtime.cu:81-92
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "engine.h"
+
+namespace bsim {
+
+// Synapse rows are read once per spike: stream them past L1 and mark them
+// evict-first in L2 (ld.global.cs) so the accumulators stay L2-resident.
+static __device__ __forceinline__ uint4 ld_stream16(const uint4 *p) { return __ldcs(p); }
+static __device__ __forceinline__ uint2 ld_stream8(const uint2 *p) { return __ldcs(p); }
+
+static __device__ __forceinline__ void red_add_u64(unsigned long long *p, unsigned long long v)
+{
+    asm volatile("red.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Phase A: LIF_brian update of a grid-stride share of the neurons.
+// Arithmetic follows LIFENeuron::update term by term with every product and
+// sum rounded on its own (no FMA contraction), as the reference's x86 build
+// evaluates it:  v = ((Cm*v + v_tmp) + i_E*C_E) + i_I*C_I.
+// ---------------------------------------------------------------------------
+template <int ACC>
+static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned long long t, int p, int cur)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int32_t *slot_ids = a.ring + (int64_t)cur * a.cap;
+    uint32_t *bm = a.bitmap + (int64_t)cur * a.W;
+    int32_t *hist = a.pop_hist ? a.pop_hist + (int64_t)(t % (unsigned long long)a.hist_len) * a.n_pops : nullptr;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < a.N; base += stride) {
+        const int64_t j = base + lane;
+        bool fired = false;
+        int pop = -1;
+        if (j < a.N) {
+            float4 st = a.state[j];
+            int refrac = __float_as_int(st.w);
+            const ClassParams *c = a.ctab + a.cls[j];
+            float inE, inI;
+            if (ACC == BSIM_ACC_EXACT) {
+                longlong2 *acc = reinterpret_cast<longlong2 *>(a.acc) + (int64_t)p * a.N;
+                longlong2 q = acc[j];
+                acc[j] = make_longlong2(0, 0);
+                const float sd = __ldg(&c->scale_down);
+                inE = __fmul_rn(__ll2float_rn(q.x), sd);
+                inI = __fmul_rn(__ll2float_rn(q.y), sd);
+            } else {
+                float2 q = reinterpret_cast<const float2 *>(a.acc)[(int64_t)p * a.N + j];
+                inE = q.x;
+                inI = q.y;
+            }
+            if (refrac > 0) {
+                refrac -= 1;  // input of this cycle is dropped
+            } else {
+                const float Cm = __ldg(&c->Cm), C_E = __ldg(&c->C_E), C_I = __ldg(&c->C_I);
+                float v = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(Cm, st.x), a.vtmp[j]), __fmul_rn(st.y, C_E)),
+                                    __fmul_rn(st.z, C_I));
+                float iE = __fmul_rn(__ldg(&c->CE), st.y);
+                float iI = __fmul_rn(__ldg(&c->CI), st.z);
+                if (v >= __ldg(&c->v_thresh)) {
+                    fired = true;
+                    refrac = __ldg(&c->refrac_time) - 1;
+                    v = __ldg(&c->v_reset);
+                } else {
+                    iE = __fadd_rn(iE, inE);
+                    iI = __fadd_rn(iI, inI);
+                }
+                st.x = v;
+                st.y = iE;
+                st.z = iI;
+            }
+            st.w = __int_as_float(refrac);
+            a.state[j] = st;
+            if (hist) pop = __ldg(&c->pop);
+        }
+        const unsigned mask = __ballot_sync(0xffffffffu, fired);
+        if (lane == 0) bm[base >> 5] = mask;
+        if (mask) {
+            const int leader = __ffs(mask) - 1;
+            int at = 0;
+            if (lane == leader) at = atomicAdd(&a.ring_cnt[cur], __popc(mask));
+            at = __shfl_sync(0xffffffffu, at, leader);
+            if (fired) {
+                slot_ids[at + __popc(mask & ((1u << lane) - 1u))] = (int32_t)j;
+                a.fire_count[j] += 1;
+            }
+            if (hist) {
+                // one atomic per (warp, population) with spikes
+                const unsigned same = __match_any_sync(0xffffffffu, fired ? pop : -1);
+                if (fired && lane == __ffs(same) - 1) atomicAdd(&hist[pop], __popc(same));
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Phase B, push: one warp per (spike, delay) segment of the source-ordered
+// rows; 16-byte streaming loads of two packed {target, weight} entries per
+// lane; exact int64 red.add into the target's E or I accumulator.
+// ---------------------------------------------------------------------------
+static __device__ __forceinline__ void push_one(unsigned long long *acc, uint32_t tgt, uint32_t wbits, float sc)
+{
+    const float w = __int_as_float(wbits);
+    const long long q = __float2ll_rn(__fmul_rn(w, sc));
+    red_add_u64(acc + 2 * (int64_t)tgt + (w >= 0.0f ? 0 : 1), (unsigned long long)q);
+}
+
+static __device__ __forceinline__ unsigned long long push_phase(const StepArgs &a, unsigned long long t, int pw,
+                                                                long long *s_cum)
+{
+    const int lane = threadIdx.x & 31;
+    const int D = a.D;
+    if (threadIdx.x < 32) {
+        long long run = 0;
+        for (int d0 = 1; d0 <= D; d0 += 32) {
+            const int d = d0 + lane;
+            long long c = 0;
+            if (d <= D && (long long)t - d >= 0) c = a.ring_cnt[(t - d) % (unsigned long long)a.R];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                long long nb = __shfl_up_sync(0xffffffffu, c, o);
+                if (lane >= o) c += nb;
+            }
+            if (d <= D) s_cum[d] = run + c;
+            run += __shfl_sync(0xffffffffu, c, 31);
+        }
+        if (lane == 0) s_cum[0] = 0;
+    }
+    __syncthreads();
+    const long long total = s_cum[D];
+    unsigned long long ev = 0;
+    unsigned long long *acc = reinterpret_cast<unsigned long long *>(a.acc) + 2 * (int64_t)pw * a.N;
+    const long long n_warps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long item = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; item < total; item += n_warps) {
+        int lo = 1, hi = D;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (s_cum[mid] > item) hi = mid;
+            else lo = mid + 1;
+        }
+        const int d = lo;
+        const long long idx = item - s_cum[d - 1];
+        const int slot = (int)((t - d) % (unsigned long long)a.R);
+        const int32_t s = a.ring[(int64_t)slot * a.cap + idx];
+        const int64_t r0 = a.row_off[(int64_t)s * D + d - 1];
+        const int64_t r1 = a.row_off[(int64_t)s * D + d];
+        const float sc = __ldg(&a.ctab[a.cls[s]].scale_up);
+        ev += (unsigned long long)(r1 - r0);
+        int64_t lo_e = r0;
+        if ((lo_e & 1) && lo_e < r1) {
+            if (lane == 0) {
+                const uint2 x = ld_stream8(a.syn + lo_e);
+                push_one(acc, x.x, x.y, sc);
+            }
+            lo_e++;
+        }
+        const int64_t npair = (r1 - lo_e) >> 1;
+        const uint4 *p4 = reinterpret_cast<const uint4 *>(a.syn + lo_e);
+        int64_t k = lane;
+        for (; k + 32 < npair; k += 64) {
+            const uint4 x0 = ld_stream16(p4 + k);
+            const uint4 x1 = ld_stream16(p4 + k + 32);
+            push_one(acc, x0.x, x0.y, sc);
+            push_one(acc, x0.z, x0.w, sc);
+            push_one(acc, x1.x, x1.y, sc);
+            push_one(acc, x1.z, x1.w, sc);
+        }
+        if (k < npair) {
+            const uint4 x0 = ld_stream16(p4 + k);
+            push_one(acc, x0.x, x0.y, sc);
+            push_one(acc, x0.z, x0.w, sc);
+        }
+        if (((r1 - lo_e) & 1) && lane == 0) {
+            const uint2 x = ld_stream8(a.syn + r1 - 1);
+            push_one(acc, x.x, x.y, sc);
+        }
+    }
+    return lane == 0 ? ev : 0ull;
+}
+
+// ---------------------------------------------------------------------------
+// Phase B, pull: one warp per target over its target-ordered row (creation
+// order), testing each source's bit in the fired bitmap of cycle t - delay.
+// EXACT: int64 fixed-point partial sums, warp-reduced (order-free).
+// ORDERED: the active weights of each 32-entry chunk are added one by one in
+// row order with warp shuffles, so the fp32 sum is formed in exactly the order
+// of the reference's loop over pSynapses.
+// ---------------------------------------------------------------------------
+template <int ACC>
+static __device__ __forceinline__ unsigned long long pull_phase(const StepArgs &a, unsigned long long t, int pw)
+{
+    const int lane = threadIdx.x & 31;
+    const long long n_warps = ((long long)gridDim.x * blockDim.x) >> 5;
+    unsigned long long ev = 0;
+    for (long long j = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < a.N; j += n_warps) {
+        const int64_t c0 = a.col_off[j], c1 = a.col_off[j + 1];
+        const float sc = (ACC == BSIM_ACC_EXACT) ? __ldg(&a.ctab[a.cls[j]].scale_up) : 0.0f;
+        long long sE = 0, sI = 0;
+        float fE = 0.0f, fI = 0.0f;
+        for (int64_t k0 = c0; k0 < c1; k0 += 32) {
+            const int64_t e = k0 + lane;
+            bool act = false;
+            float w = 0.0f;
+            if (e < c1) {
+                const uint32_t s = __ldcs(a.csc_src + e);
+                const int d = (int)__ldcs(a.csc_d + e) + 1;
+                w = __ldcs(a.csc_w + e);
+                if ((long long)t - d >= 0) {
+                    const int slot = (int)((t - d) % (unsigned long long)a.R);
+                    act = (a.bitmap[(int64_t)slot * a.W + (s >> 5)] >> (s & 31)) & 1u;
+                }
+            }
+            unsigned m = __ballot_sync(0xffffffffu, act);
+            ev += __popc(m);
+            if (ACC == BSIM_ACC_EXACT) {
+                if (act) {
+                    const long long q = __float2ll_rn(__fmul_rn(w, sc));
+                    if (w >= 0.0f) sE += q;
+                    else sI += q;
+                }
+            } else {
+                while (m) {
+                    const int b = __ffs(m) - 1;
+                    const float wb = __shfl_sync(0xffffffffu, w, b);
+                    if (wb >= 0.0f) fE = __fadd_rn(fE, wb);
+                    else fI = __fadd_rn(fI, wb);
+                    m &= m - 1;
+                }
+            }
+        }
+        if (ACC == BSIM_ACC_EXACT) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                sE += __shfl_xor_sync(0xffffffffu, sE, o);
+                sI += __shfl_xor_sync(0xffffffffu, sI, o);
+            }
+            if (lane == 0) reinterpret_cast<longlong2 *>(a.acc)[(int64_t)pw * a.N + j] = make_longlong2(sE, sI);
+        } else {
+            if (lane == 0) reinterpret_cast<float2 *>(a.acc)[(int64_t)pw * a.N + j] = make_float2(fE, fI);
+        }
+    }
+    return lane == 0 ? ev : 0ull;
+}
+
+// Copies the complete ring slot of cycle t-1 into the raster recording.
+static __device__ __forceinline__ void record_phase(const StepArgs &a, unsigned long long t)
+{
+    if (!a.rec || t == 0) return;
+    RecCtl rc;
+    {
+        const volatile RecCtl *v = a.rec;
+        rc.next = v->next;
+        rc.t0 = v->t0;
+        rc.steps = v->steps;
+        rc.cap = v->cap;
+    }
+    const long long ts = (long long)t - 1;
+    const long long k = ts - rc.t0;
+    if (k < 0 || k >= rc.steps || rc.next != ts) return;
+    const int slot = (int)(ts % a.R);
+    const int64_t n = a.ring_cnt[slot];
+    const int64_t base = a.rec_off[k];
+    int64_t room = rc.cap - base;
+    if (room < 0) room = 0;
+    const int64_t ncopy = n < room ? n : room;
+    const int32_t *src = a.ring + (int64_t)slot * a.cap;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ncopy; i += (int64_t)gridDim.x * blockDim.x)
+        a.rec_ids[base + i] = src[i];
+}
+
+template <int ACC>
+__global__ void __launch_bounds__(512) step_kernel(const StepArgs a)
+{
+    __shared__ long long s_cum[BSIM_MAX_DELAY + 1];
+    __shared__ unsigned long long s_ev;
+    const unsigned long long t = *reinterpret_cast<volatile unsigned long long *>(a.step_ctr);
+    const int p = (int)(t & 1ull);
+    const int cur = (int)(t % (unsigned long long)a.R);
+    if (threadIdx.x == 0) s_ev = 0;
+    __syncthreads();
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        // slot t+1 is neither written (LIF writes slot t) nor read (delivery reads t-1..t-D) now
+        a.ring_cnt[(t + 1) % (unsigned long long)a.R] = 0;
+    }
+    if (a.pop_hist) {
+        int32_t *nxt = a.pop_hist + (int64_t)((t + 1) % (unsigned long long)a.hist_len) * a.n_pops;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_pops; i += gridDim.x * blockDim.x) nxt[i] = 0;
+    }
+    lif_phase<ACC>(a, t, p, cur);
+    record_phase(a, t);
+    unsigned long long ev;
+    const int dm = a.deliv_sel ? *a.deliv_sel : a.delivery;
+    if (ACC == BSIM_ACC_ORDERED || dm == BSIM_DELIVERY_PULL) ev = pull_phase<ACC>(a, t, p ^ 1);
+    else ev = push_phase(a, t, p ^ 1, s_cum);
+    if (ev) atomicAdd(&s_ev, ev);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (s_ev) atomicAdd(a.events, s_ev);
+        __threadfence();
+        const unsigned v = atomicAdd(a.ticket, 1u);
+        if (v == gridDim.x - 1) {
+            // every other block has finished this cycle: advance the cycle
+            if (a.rec && t > 0) {
+                RecCtl *rc = a.rec;
+                const long long k = (long long)t - 1 - rc->t0;
+                if (k >= 0 && k < rc->steps && rc->next == (long long)t - 1) {
+                    const int64_t n = a.ring_cnt[(t - 1) % (unsigned long long)a.R];
+                    a.rec_off[k + 1] = a.rec_off[k] + n;
+                    rc->next = (long long)t;
+                }
+            }
+            *a.ticket = 0u;
+            *a.step_ctr = t + 1;
+            __threadfence();
+        }
+    }
+}
+
+// Records the last completed cycle (run after a batch of steps, before reading the raster).
+__global__ void record_flush_kernel(const StepArgs a)
+{
+    const unsigned long long t = *a.step_ctr;  // first cycle not yet run
+    if (t == 0 || !a.rec) return;
+    const RecCtl rc = *a.rec;
+    const long long ts = (long long)t - 1;
+    const long long k = ts - rc.t0;
+    if (k < 0 || k >= rc.steps || rc.next != ts) return;
+    const int slot = (int)(ts % a.R);
+    const int64_t n = a.ring_cnt[slot];
+    const int64_t base = a.rec_off[k];
+    int64_t room = rc.cap - base;
+    if (room < 0) room = 0;
+    const int64_t ncopy = n < room ? n : room;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ncopy; i += (int64_t)gridDim.x * blockDim.x)
+        a.rec_ids[base + i] = a.ring[(int64_t)slot * a.cap + i];
+    __syncthreads();
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.rec_off[k + 1] = base + n;
+        a.rec->next = ts + 1;
+    }
+}
+
+cudaError_t launch_step(Engine &e)
+{
+    if (e.opt.accumulate == BSIM_ACC_ORDERED)
+        step_kernel<BSIM_ACC_ORDERED><<<e.grid, e.block, 0, e.stream>>>(e.a);
+    else
+        step_kernel<BSIM_ACC_EXACT><<<e.grid, e.block, 0, e.stream>>>(e.a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_record_flush(Engine &e)
+{
+    record_flush_kernel<<<1, 256, 0, e.stream>>>(e.a);
+    return cudaGetLastError();
+}
+
+cudaError_t step_occupancy(int block, int accumulate, int *blocks_per_sm)
+{
+    if (accumulate == BSIM_ACC_ORDERED)
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<BSIM_ACC_ORDERED>, block, 0);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<BSIM_ACC_EXACT>, block, 0);
+}
+
+}  // namespace bsim

@@ -1,0 +1,189 @@
+/*
+ * bsim_b200 — C ABI of the B200 (sm_100a) engine behind BSim's single-GPU
+ * simulation step for LIF_brian neurons and static delayed synapses.
+ *
+ * The reference drives this path through per-type function-pointer tables
+ * (src/utils/TypeFunc.h:11-21) filled with cudaAllocLIFE / cudaUpdateLIFE /
+ * cudaUpdateStatic and friends, and through process-wide __device__ globals
+ * (src/gpu_utils/runtime.cu:28-63). This ABI replaces those with an opaque
+ * engine handle, plain pointers and sizes, and int status codes (the reference
+ * calls exit() on CUDA errors, src/third_party/cuda/helper_cuda.h:985-999).
+ *
+ * Units are SI (V, s, F, A), as in the reference. Inhibition is a negative
+ * weight. All functions return BSIM_OK (0) or a negative BSIM_ERR_* code.
+ * Host pointers are plain host memory unless a name ends in _dev.
+ */
+#ifndef BSIM_B200_H
+#define BSIM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BSIM_OK 0
+#define BSIM_ERR_ARG (-1)      /* invalid argument or size */
+#define BSIM_ERR_CUDA (-2)     /* CUDA runtime error (message in bsim_last_error) */
+#define BSIM_ERR_DEVICE (-3)   /* device-side error flag raised (bad index, overflow, timeout) */
+#define BSIM_ERR_DELAY (-4)    /* a synapse delay rounds to 0 steps or above BSIM_MAX_DELAY */
+#define BSIM_ERR_NOMEM (-5)    /* device or host allocation failed */
+#define BSIM_ERR_STATE (-6)    /* call not valid in the engine's current state */
+#define BSIM_ERR_LIMIT (-7)    /* network exceeds a documented engine limit */
+
+#define BSIM_MAX_DELAY 1024    /* delays are 1..BSIM_MAX_DELAY steps */
+#define BSIM_MAX_CLASSES 65535 /* distinct folded LIF parameter tuples per engine */
+
+/* How one step's synaptic input is summed per target neuron. */
+#define BSIM_ACC_EXACT 0   /* exact int64 fixed point (quantum 2^-qexp per network): the sum is
+                              independent of delivery order, so push, pull, batched and
+                              predictor-scheduled runs give bit-identical results; equal to the
+                              reference's sequential fp32 sum whenever a target receives at most
+                              two same-sign inputs in a step, else the correctly rounded sum. */
+#define BSIM_ACC_ORDERED 1 /* sequential fp32 sums in synapse creation order, the order of the
+                              reference's StaticSynapse::update loop (src/net/Network.cpp:320-325):
+                              bit-identical to the reference CPU simulator. Pull delivery only. */
+
+#define BSIM_DELIVERY_PUSH 0 /* source-ordered rows, one warp per (spike, delay) segment */
+#define BSIM_DELIVERY_PULL 1 /* target-ordered rows scanned against per-step fired bitmaps */
+#define BSIM_DELIVERY_AUTO 2 /* per step, by the firing predictor (EXACT accumulation only) */
+
+typedef struct bsim_engine bsim_engine;
+
+typedef struct bsim_options {
+    int32_t device;        /* CUDA device ordinal (the reference hard-codes 0, SingleGPUSimulator.cu:83) */
+    int32_t accumulate;    /* BSIM_ACC_* */
+    int32_t delivery;      /* BSIM_DELIVERY_* */
+    int32_t build_pull;    /* also build the target-ordered copy (forced on for PULL/AUTO/ORDERED) */
+    int32_t graph_steps;   /* steps captured per CUDA graph by bsim_run (0: plain launches) */
+    int32_t block_threads; /* threads per block of the step kernel (0: autotuned) */
+    int32_t grid_blocks;   /* blocks of the step kernel (0: autotuned) */
+    int32_t reserved[9];
+} bsim_options;
+
+/* Parameters of one generated network (see bsim_create_generated). */
+typedef struct bsim_gen_spec {
+    uint64_t seed;
+    int32_t n_pop;         /* populations */
+    int32_t pop_size;      /* neurons per population */
+    float p_conn;          /* Bernoulli connection probability of each projection */
+    float remote_frac;     /* fraction of populations with one extra remote projection */
+    int32_t max_delay;     /* delays U{1..max_delay} steps */
+    float exc_frac;        /* probability that a synapse is excitatory */
+    float w_max;           /* excitatory weight U[0, w_max) */
+    float inh_scale;       /* inhibitory weight -U[0, inh_scale * w_max) */
+    float i_min, i_max;    /* i_offset U[i_min, i_max) per neuron */
+    float v_init_lo, v_init_hi; /* v_init U[lo, hi) per neuron */
+    /* LIFENeuron parameters shared by all neurons (constructor order minus v_init, i_offset) */
+    float v_rest, v_reset, cm, tau_m, tau_refrac, tau_syn_E, tau_syn_I, v_thresh;
+} bsim_gen_spec;
+
+typedef struct bsim_info {
+    int64_t n_neurons;
+    int64_t n_synapses;
+    int32_t max_delay;       /* D, steps */
+    int32_t n_instances;     /* independent networks packed in the engine */
+    int32_t n_classes;       /* distinct folded parameter tuples */
+    int32_t n_pops;          /* populations (spike statistics granularity) */
+    int64_t steps_done;      /* simulated cycles so far */
+    uint64_t events_total;   /* synaptic events delivered so far */
+    int64_t device_bytes;    /* device memory held by the engine */
+    int32_t grid_blocks, block_threads;
+    int32_t accumulate, delivery;
+    int32_t sm_count;
+    int32_t reserved[7];
+} bsim_info;
+
+/* Fills *opt with defaults: EXACT accumulation, PUSH delivery, graphs of 64 steps. */
+int bsim_options_default(bsim_options *opt);
+
+/* Builds an engine from flat host arrays and uploads it.
+ * Replaces Network::buildNetwork (src/net/BuildNetwork.cpp:36-205), copyNetworkToGPU
+ * (src/gpu_utils/gpu_net_copy.cu:8-109), alloc_buffers (src/gpu_utils/GBuffers.cu:9-56),
+ * the LIFE allocators cudaAllocLIFE/allocLIFE (src/neuron/lif/GLIFENeurons.cu:6,
+ * GLIFENeurons.cpp:8-30) and the neuron half of Network::reset (LIFENeuron::reset,
+ * src/neuron/lif/LIFENeuron.cpp:68-112, folded here in fp32 on the host exactly as there).
+ *   params      [n][10] LIFENeuron constructor arguments per neuron, global id order:
+ *               v_init, v_rest, v_reset, cm, tau_m, tau_refrac, tau_syn_E, tau_syn_I, v_thresh, i_offset
+ *   pop         [n] population of each neuron (statistics only; may be NULL = one population)
+ *   instance    [n] independent network of each neuron (may be NULL = one network); a
+ *               synapse must not join two instances
+ *   src, dst    [s] neuron ids, synapses in creation (Network::connect) order
+ *   weight      [s] weights after StaticSynapse::reset (see bsim_synapse_reset)
+ *   delay_steps [s] 1..BSIM_MAX_DELAY
+ */
+int bsim_create(const float *params, int64_t n, const int32_t *pop, const int32_t *instance,
+                const int32_t *src, const int32_t *dst, const float *weight, const int32_t *delay_steps,
+                int64_t s, float dt, const bsim_options *opt, bsim_engine **out);
+
+/* Builds an engine for one or more generated networks directly on the device
+ * (no host synapse arrays). Network k's neurons follow network k-1's. */
+int bsim_create_generated(const bsim_gen_spec *specs, int32_t n_specs, float dt, const bsim_options *opt,
+                          bsim_engine **out);
+
+/* Host-side generator: sizes, then the flat arrays bsim_create takes, for one spec.
+ * params is [n][10] in LIFENeuron constructor order. Identical to the device builder. */
+int bsim_gen_count(const bsim_gen_spec *spec, int64_t *n, int64_t *s);
+int bsim_gen_host(const bsim_gen_spec *spec, float *params, int32_t *pop, int32_t *src, int32_t *dst,
+                  float *weight, int32_t *delay_steps);
+
+/* StaticSynapse::reset (src/synapse/static/StaticSynapse.cpp:43-54): delays in seconds to
+ * whole steps, and the weight decay exp(-(delay - dt*steps)/tau) applied when the delay is
+ * not a multiple of dt. Host only. */
+int bsim_synapse_reset(const float *delay_s, const float *weight, const float *tau_syn, int64_t s, float dt,
+                       int32_t *delay_steps, float *weight_out);
+
+/* Advances the simulation by `steps` cycles on the engine's stream, without host
+ * synchronisation between steps; returns after the device has finished.
+ * Replaces the step loop of SingleGPUSimulator::run (src/sim/SingleGPUSimulator.cu:146-245):
+ * cudaUpdateLIFE (src/gpu_utils/gpu_func.cu:44-51) + cudaUpdateStatic (:67-74) +
+ * update_time (src/gpu_utils/runtime.cu:81-92) fused into one launch per step. */
+int bsim_run(bsim_engine *e, int64_t steps);
+
+/* Like bsim_run but only enqueues the work (no final synchronisation). */
+int bsim_run_async(bsim_engine *e, int64_t steps);
+int bsim_sync(bsim_engine *e);
+
+/* Records the fired ids of the next `max_steps` cycles into a device buffer of
+ * `capacity` ids (the reference's LOG_DATA GSim.log, SingleGPUSimulator.cu:209-237,
+ * without a host sync per step). Calling it again restarts the recording. */
+int bsim_record(bsim_engine *e, int64_t max_steps, int64_t capacity);
+
+/* Copies the recording out: step_off [n_steps+1], ids in step order (each step's ids
+ * ascending). *n_steps receives the recorded steps. BSIM_ERR_LIMIT if the buffer overflowed. */
+int bsim_read_raster(bsim_engine *e, int64_t *step_off, int32_t *ids, int64_t ids_cap, int64_t *n_steps);
+
+/* Neuron state: v, i_E, i_I, refrac_step per neuron (cudaFetchLIFE,
+ * src/neuron/lif/GLIFENeurons.cu:29-40). Any pointer may be NULL. */
+int bsim_read_state(bsim_engine *e, float *v, float *i_E, float *i_I, int32_t *refrac_step);
+
+/* Overwrites the neuron state from host arrays (the state half of copyNetworkToGPU,
+ * src/gpu_utils/gpu_net_copy.cu:8-109, as restored by single_run). NULL leaves a field. */
+int bsim_write_state(bsim_engine *e, const float *v, const float *i_E, const float *i_I, const int32_t *refrac_step);
+
+/* The CUDA stream (cudaStream_t) all of the engine's work is enqueued on. */
+int bsim_get_stream(bsim_engine *e, void **stream);
+
+/* Spikes per neuron since creation (FireInfo "count", src/sim/SingleGPUSimulator.cu:263-282). */
+int bsim_read_fire_count(bsim_engine *e, int32_t *count);
+
+/* Spike count of each population over the last `steps` recorded cycles
+ * ([steps][n_pops], oldest first; at most the predictor history length). */
+int bsim_read_pop_counts(bsim_engine *e, int32_t *counts, int32_t steps);
+
+int bsim_get_info(bsim_engine *e, bsim_info *info);
+
+/* Per-network fixed-point exponent used by BSIM_ACC_EXACT ([n_instances]). */
+int bsim_get_qexp(bsim_engine *e, int32_t *qexp);
+
+/* Frees the engine (freeGPUNetwork + free_buffers, src/gpu_utils/gpu_net_copy.cu:134-191). */
+int bsim_destroy(bsim_engine *e);
+
+/* Text of the last error raised in this thread. */
+const char *bsim_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BSIM_B200_H */
