@@ -41,6 +41,9 @@ def workload(name, seed):
     if name == "plain_1m":
         specs, _ = W.plain_1m(seed)
         desc = "100 x 10,000 LIF_brian CUBA, ~500 Hz, delays U{1..6}, p=0.1 chain + 20% remote"
+    elif name == "plain_quarter":
+        specs = [W.cuba(25, 10000, 500, 6, seed, i_max=30e-9)]
+        desc = "25 x 10,000 LIF_brian CUBA, ~500 Hz, delays U{1..6} (profiling size: 2.4 GB of rows)"
     elif name == "standard_cpu":
         specs, _ = W.standard_cpu(seed)
         desc = "10 x 1,000 LIF_brian CUBA, ~100 Hz, delays U{1..6}"
@@ -213,6 +216,8 @@ def main():
     ap.add_argument("--config", default="plain_1m")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--delivery", default="push", choices=["push", "pull"])
+    ap.add_argument("--settle", type=int, default=1000,
+                    help="untimed cycles run at set-up so the network leaves its start-up transient")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -241,6 +246,7 @@ def main():
     info = eng.info()
     N, S = info.n_neurons, info.n_synapses
 
+    eng.run(args.settle)   # set-up: leave the start-up transient (rates settle within ~0.1 s)
     eng.run(args.warmup)
     stream = torch.cuda.ExternalStream(eng.stream(), device=local)
     e0 = torch.cuda.Event(enable_timing=True)
@@ -341,7 +347,7 @@ def main():
                            "delivery": args.delivery, "accumulate": "exact int64",
                            "parallelism": "replicas x%d (independent networks, no collective)" % world,
                            "l2": "inputs larger than L2 (%.1f GB of synapse rows per GPU)" % (S * 8 / 1e9),
-                           "build_seconds": t_build},
+                           "build_seconds": t_build, "settle_steps": args.settle},
                 "realtime_factor": rtf, "spikes_per_step": spikes_all / args.steps / world,
                 "events_per_step": events_all / args.steps / world,
                 "mean_rate_hz": spikes_all / n_all / (args.steps * DT),

@@ -128,77 +128,130 @@ static __device__ __forceinline__ void push_one(unsigned long long *acc, uint32_
     red_add_u64(acc + 2 * (int64_t)tgt + (w >= 0.0f ? 0 : 1), (unsigned long long)q);
 }
 
-static __device__ __forceinline__ unsigned long long push_phase(const StepArgs &a, unsigned long long t, int pw,
-                                                                long long *s_cum)
+// (spike, delay) segments whose metadata one warp resolves at once
+#define PUSH_CHUNK 8
+#define MAX_WARPS 16
+
+struct PushSeg {
+    long long incl;  // inclusive prefix of the chunk's pair counts
+    int64_t p0;      // first entry of the segment's first 16-byte pair
+    float sc;        // 2^qexp of the segment's network
+};
+
+// s_cum[d] = spikes of cycles t-1 .. t-d (the push work items of delays 1..d).
+// Run by warp 0 before the LIF phase, so its loads overlap the neuron update;
+// the caller's __syncthreads publishes it.
+static __device__ __forceinline__ void delay_window_prefix(const StepArgs &a, unsigned long long t, long long *s_cum)
 {
     const int lane = threadIdx.x & 31;
     const int D = a.D;
-    if (threadIdx.x < 32) {
-        long long run = 0;
-        for (int d0 = 1; d0 <= D; d0 += 32) {
-            const int d = d0 + lane;
-            long long c = 0;
-            if (d <= D && (long long)t - d >= 0) c = a.ring_cnt[(t - d) % (unsigned long long)a.R];
+    long long run = 0;
+    for (int d0 = 1; d0 <= D; d0 += 32) {
+        const int d = d0 + lane;
+        long long c = 0;
+        if (d <= D && (long long)t - d >= 0) c = a.ring_cnt[(t - d) % (unsigned long long)a.R];
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                long long nb = __shfl_up_sync(0xffffffffu, c, o);
-                if (lane >= o) c += nb;
-            }
-            if (d <= D) s_cum[d] = run + c;
-            run += __shfl_sync(0xffffffffu, c, 31);
+        for (int o = 1; o < 32; o <<= 1) {
+            long long nb = __shfl_up_sync(0xffffffffu, c, o);
+            if (lane >= o) c += nb;
         }
-        if (lane == 0) s_cum[0] = 0;
+        if (d <= D) s_cum[d] = run + c;
+        run += __shfl_sync(0xffffffffu, c, 31);
     }
-    __syncthreads();
+    if (lane == 0) s_cum[0] = 0;
+}
+
+static __device__ __forceinline__ unsigned long long push_phase(const StepArgs &a, unsigned long long t, int pw,
+                                                                const long long *s_cum, PushSeg *s_seg)
+{
+    const int lane = threadIdx.x & 31;
+    const int D = a.D;
     const long long total = s_cum[D];
     unsigned long long ev = 0;
     unsigned long long *acc = reinterpret_cast<unsigned long long *>(a.acc) + 2 * (int64_t)pw * a.N;
     const long long n_warps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long item = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; item < total; item += n_warps) {
-        int lo = 1, hi = D;
-        while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (s_cum[mid] > item) hi = mid;
-            else lo = mid + 1;
-        }
-        const int d = lo;
-        const long long idx = item - s_cum[d - 1];
-        const int slot = (int)((t - d) % (unsigned long long)a.R);
-        const int32_t s = a.ring[(int64_t)slot * a.cap + idx];
-        const int64_t r0 = a.row_off[(int64_t)s * D + d - 1];
-        const int64_t r1 = a.row_off[(int64_t)s * D + d];
-        const float sc = __ldg(&a.ctab[a.cls[s]].scale_up);
-        ev += (unsigned long long)(r1 - r0);
-        int64_t lo_e = r0;
-        if ((lo_e & 1) && lo_e < r1) {
-            if (lane == 0) {
-                const uint2 x = ld_stream8(a.syn + lo_e);
-                push_one(acc, x.x, x.y, sc);
+    const long long n_chunks = (total + PUSH_CHUNK - 1) / PUSH_CHUNK;
+    for (long long ch = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; ch < n_chunks; ch += n_warps) {
+        // Lanes 0..PUSH_CHUNK-1 each resolve one (spike, delay) segment: its row
+        // [r0, r1), split into an odd head entry, 16-byte pairs [p0, p0 + 2*np)
+        // and an odd tail entry.
+        int64_t r0 = 0, r1 = 0;
+        float sc = 0.0f;
+        const long long item = ch * PUSH_CHUNK + lane;
+        if (lane < PUSH_CHUNK && item < total) {
+            int lo = 1, hi = D;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (s_cum[mid] > item) hi = mid;
+                else lo = mid + 1;
             }
-            lo_e++;
+            const int d = lo;
+            const int slot = (int)((t - d) % (unsigned long long)a.R);
+            const int32_t s = a.ring[(int64_t)slot * a.cap + (item - s_cum[d - 1])];
+            r0 = a.row_off[(int64_t)s * D + d - 1];
+            r1 = a.row_off[(int64_t)s * D + d];
+            sc = __ldg(&a.ctab[a.cls[s]].scale_up);
+            ev += (unsigned long long)(r1 - r0);
         }
-        const int64_t npair = (r1 - lo_e) >> 1;
-        const uint4 *p4 = reinterpret_cast<const uint4 *>(a.syn + lo_e);
-        int64_t k = lane;
-        for (; k + 32 < npair; k += 64) {
-            const uint4 x0 = ld_stream16(p4 + k);
-            const uint4 x1 = ld_stream16(p4 + k + 32);
-            push_one(acc, x0.x, x0.y, sc);
-            push_one(acc, x0.z, x0.w, sc);
-            push_one(acc, x1.x, x1.y, sc);
-            push_one(acc, x1.z, x1.w, sc);
+        const int64_t p0 = (r0 & 1) && r0 < r1 ? r0 + 1 : r0;  // first entry of the first pair
+        const long long np = (r1 - p0) >> 1;
+        const bool head = p0 != r0, tail = ((r1 - p0) & 1) != 0;
+        // inclusive prefix of pair counts over the chunk's segments
+        long long incl = np;
+#pragma unroll
+        for (int o = 1; o < PUSH_CHUNK; o <<= 1) {
+            const long long nb = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += nb;
         }
-        if (k < npair) {
-            const uint4 x0 = ld_stream16(p4 + k);
-            push_one(acc, x0.x, x0.y, sc);
-            push_one(acc, x0.z, x0.w, sc);
+        // the chunk's segment table, in this warp's slice of shared memory
+        PushSeg *seg = s_seg + (threadIdx.x >> 5) * PUSH_CHUNK;
+        __syncwarp();
+        if (lane < PUSH_CHUNK) {
+            seg[lane].incl = incl;
+            seg[lane].p0 = p0;
+            seg[lane].sc = sc;
         }
-        if (((r1 - lo_e) & 1) && lane == 0) {
-            const uint2 x = ld_stream8(a.syn + r1 - 1);
-            push_one(acc, x.x, x.y, sc);
+        __syncwarp();
+        const long long total_pairs = __shfl_sync(0xffffffffu, incl, PUSH_CHUNK - 1);
+        // head / tail single entries: lane L handles segment L>>1, head if L even
+        {
+            const int k = lane >> 1;
+            const bool want_head = (lane & 1) == 0;
+            const bool hk = __shfl_sync(0xffffffffu, head, k & (PUSH_CHUNK - 1));
+            const bool tk = __shfl_sync(0xffffffffu, tail, k & (PUSH_CHUNK - 1));
+            const int64_t rk0 = __shfl_sync(0xffffffffu, r0, k & (PUSH_CHUNK - 1));
+            const int64_t rk1 = __shfl_sync(0xffffffffu, r1, k & (PUSH_CHUNK - 1));
+            const float sk = __shfl_sync(0xffffffffu, sc, k & (PUSH_CHUNK - 1));
+            if (k < PUSH_CHUNK && ((want_head && hk) || (!want_head && tk))) {
+                const uint2 x = ld_stream8(a.syn + (want_head ? rk0 : rk1 - 1));
+                push_one(acc, x.x, x.y, sk);
+            }
+        }
+        // the pairs of all segments as one flat range, four loads in flight per lane
+        for (long long pb = 0; pb < total_pairs; pb += 4 * 32) {
+            uint4 x[4];
+            float xs[4];
+            bool ok[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const long long p = pb + u * 32 + lane;
+                ok[u] = p < total_pairs;
+                int k = 0;
+                while (k < PUSH_CHUNK - 1 && p >= seg[k].incl) k++;
+                const long long excl = k == 0 ? 0 : seg[k - 1].incl;
+                xs[u] = seg[k].sc;
+                if (ok[u]) x[u] = ld_stream16(reinterpret_cast<const uint4 *>(a.syn + seg[k].p0) + (p - excl));
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                if (ok[u]) {
+                    push_one(acc, x[u].x, x[u].y, xs[u]);
+                    push_one(acc, x[u].z, x[u].w, xs[u]);
+                }
+            }
         }
     }
-    return lane == 0 ? ev : 0ull;
+    return ev;
 }
 
 // ---------------------------------------------------------------------------
@@ -295,12 +348,15 @@ template <int ACC>
 __global__ void __launch_bounds__(512) step_kernel(const StepArgs a)
 {
     __shared__ long long s_cum[BSIM_MAX_DELAY + 1];
+    __shared__ PushSeg s_seg[MAX_WARPS * PUSH_CHUNK];
     __shared__ unsigned long long s_ev;
     const unsigned long long t = *reinterpret_cast<volatile unsigned long long *>(a.step_ctr);
     const int p = (int)(t & 1ull);
     const int cur = (int)(t % (unsigned long long)a.R);
+    const int dm = a.deliv_sel ? *a.deliv_sel : a.delivery;
+    const bool push = ACC != BSIM_ACC_ORDERED && dm != BSIM_DELIVERY_PULL;
     if (threadIdx.x == 0) s_ev = 0;
-    __syncthreads();
+    if (push && threadIdx.x < 32) delay_window_prefix(a, t, s_cum);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         // slot t+1 is neither written (LIF writes slot t) nor read (delivery reads t-1..t-D) now
         a.ring_cnt[(t + 1) % (unsigned long long)a.R] = 0;
@@ -311,10 +367,10 @@ __global__ void __launch_bounds__(512) step_kernel(const StepArgs a)
     }
     lif_phase<ACC>(a, t, p, cur);
     record_phase(a, t);
+    __syncthreads();  // publishes s_cum and s_ev
     unsigned long long ev;
-    const int dm = a.deliv_sel ? *a.deliv_sel : a.delivery;
-    if (ACC == BSIM_ACC_ORDERED || dm == BSIM_DELIVERY_PULL) ev = pull_phase<ACC>(a, t, p ^ 1);
-    else ev = push_phase(a, t, p ^ 1, s_cum);
+    if (push) ev = push_phase(a, t, p ^ 1, s_cum, s_seg);
+    else ev = pull_phase<ACC>(a, t, p ^ 1);
     if (ev) atomicAdd(&s_ev, ev);
     __syncthreads();
     if (threadIdx.x == 0) {

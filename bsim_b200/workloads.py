@@ -10,9 +10,13 @@ steps, dt = 0.1 ms, i_offset U[0, i_max) per neuron and v_init U[-65, -50) mV.
 
 The mean firing rate is set by i_offset (the recurrent input is balanced on
 average). A 2 ms refractory period caps a LIF_brian neuron at 1/(20 steps) =
-500 Hz, so the 500 Hz and 2 kHz presets shorten it (0.5 ms, 0.2 ms); the
-i_max values were calibrated with the CPU oracle on 10 x 1,000-neuron nets and
-hold on 4 x 10,000-neuron nets within a few percent.
+500 Hz, so the 500 Hz and 2 kHz presets shorten it (0.5 ms, 0.2 ms). The
+i_max values were calibrated by simulation (mean rate over steps 1,000-2,000):
+the presets on 10 x 1,000-neuron nets with the CPU oracle, and the large
+configurations on the GPU at full size. In the 100-population chain the
+recurrent inhibition silences a few populations (per-population rates span
+0-1,280 Hz), so a larger i_offset raises the mean only slowly: i_max = 30 nA
+gives ~430 Hz there.
 """
 import numpy as np
 
@@ -21,14 +25,14 @@ from . import gen_spec
 DT = 1.0e-4
 W_MAX = 1.0e-10
 
-# rate (Hz) -> (tau_refrac s, i_max A)
+# rate (Hz) -> (tau_refrac s, i_max A), calibrated on 10 x 1,000-neuron nets
 RATE_PRESETS = {100: (2.0e-3, 3.2e-9), 500: (0.5e-3, 17.5e-9), 2000: (0.2e-3, 50.0e-9)}
 
 
-def cuba(n_pop, pop_size, rate_hz=100, max_delay=6, seed=1, w_max=W_MAX):
+def cuba(n_pop, pop_size, rate_hz=100, max_delay=6, seed=1, w_max=W_MAX, i_max=None):
     tref, imax = RATE_PRESETS[rate_hz]
     return gen_spec(seed=seed, n_pop=n_pop, pop_size=pop_size, max_delay=max_delay, w_max=w_max,
-                    i_min=0.0, i_max=imax, tau_refrac=tref)
+                    i_min=0.0, i_max=imax if i_max is None else i_max, tau_refrac=tref)
 
 
 def standard_cpu(seed=1):
@@ -37,13 +41,15 @@ def standard_cpu(seed=1):
 
 
 def plain_1m(seed=1):
-    """100 populations x 10,000 neurons (1e6 neurons, ~1.19e9 synapses), ~500 Hz, delays U{1..6}, 1 s."""
-    return [cuba(100, 10000, 500, 6, seed)], 10000
+    """100 populations x 10,000 neurons (1e6 neurons, ~1.19e9 synapses), ~430 Hz (the 500 Hz
+    preset's refractory period, i_max = 30 nA), delays U{1..6}, 1 s."""
+    return [cuba(100, 10000, 500, 6, seed, i_max=30e-9)], 10000
 
 
 def dense_1m(seed=1):
-    """50 populations x 20,000 neurons (~2.36e9 synapses), ~2 kHz, delays U{1..50}, 0.5 s."""
-    return [cuba(50, 20000, 2000, 50, seed)], 5000
+    """50 populations x 20,000 neurons (~2.36e9 synapses), ~2 kHz (i_max = 62.5 nA),
+    delays U{1..50}, 0.5 s."""
+    return [cuba(50, 20000, 2000, 50, seed, i_max=62.5e-9)], 5000
 
 
 def batched(n_nets=256, seed=1):
