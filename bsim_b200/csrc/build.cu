@@ -32,6 +32,9 @@ static int fail(int code, const std::string &msg)
     return code;
 }
 
+// Lets the other translation units report through bsim_last_error().
+int record_error(int code, const std::string &msg) { return fail(code, msg); }
+
 #define CK(call)                                                                                    \
     do {                                                                                            \
         cudaError_t _e = (call);                                                                    \

@@ -428,6 +428,13 @@ cudaError_t launch_step(Engine &e)
     return cudaGetLastError();
 }
 
+// One step on explicit arguments (used by the allocation-free entry point).
+cudaError_t launch_step_exact(const StepArgs &a, int grid, int block, cudaStream_t stream)
+{
+    step_kernel<BSIM_ACC_EXACT><<<grid, block, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_record_flush(Engine &e)
 {
     record_flush_kernel<<<1, 256, 0, e.stream>>>(e.a);

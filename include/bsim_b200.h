@@ -182,6 +182,53 @@ int bsim_destroy(bsim_engine *e);
 /* Text of the last error raised in this thread. */
 const char *bsim_last_error(void);
 
+/* ---- Allocation-free step -------------------------------------------------
+ * No counterpart in the reference: it has no entry point of this kind.
+ *
+ * For callers that cannot allocate device memory: a host application that owns
+ * the GPU's memory through its own pool and hands its plug-ins ready-made
+ * buffers (a cudaMalloc would bypass its accounting, and cudaMalloc/cudaFree can
+ * synchronise the whole device), a real-time loop that cannot take an
+ * allocation's latency or implicit synchronisation, or a process that has
+ * already reserved the remaining device memory.
+ *
+ * The caller passes every input and output as device pointers; the step's
+ * working memory (input accumulators, fire ring, fired bitmaps, counters) is a
+ * fixed array of about 3.4 MB inside the library, held by every GPU that loads
+ * the library until the process exits. Limits: n <= BSIM_NOALLOC_MAX_NEURONS,
+ * max_delay <= BSIM_NOALLOC_MAX_DELAY; larger sizes return BSIM_ERR_LIMIT. No
+ * cudaMalloc, cudaFree or other allocating routine is called.
+ *
+ * The first call on a device looks the array up (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture.
+ * All calls on a device share the array and each call clears it first: calls
+ * whose GPU work overlaps (other streams, unordered threads) race on it.
+ *
+ * Each call runs `steps` cycles with EXACT accumulation and push delivery, on
+ * `stream` (a cudaStream_t, NULL = legacy default stream), starting with no
+ * spikes in flight, and returns once the work is enqueued.
+ *   state_dev      [n] float4 {v, i_E, i_I, refrac_step bit pattern}, in/out, 16-byte aligned
+ *   vtmp_dev       [n] (i_offset * rm + v_rest) * (1 - Cm), as LIFENeuron::reset folds it
+ *   cls_dev        [n] class of each neuron
+ *   ctab_dev       [classes] folded constants, scale_up = 2^qexp, scale_down = 2^-qexp
+ *   row_off_dev    [n * max_delay + 1] rows by (source, delay - 1), delay-minor
+ *   syn_dev        [2 * entries] {target id, weight bit pattern} per entry, 16-byte aligned
+ *   fire_count_dev [n] incremented by each neuron's spikes
+ */
+#define BSIM_NOALLOC_MAX_NEURONS 32768
+#define BSIM_NOALLOC_MAX_DELAY 16
+
+typedef struct bsim_class_params {
+    float Cm, CE, CI, C_E, C_I, v_thresh, v_reset;
+    int32_t refrac_time;
+    float scale_up, scale_down;
+    int32_t pop, inst;
+} bsim_class_params;
+
+int bsim_run_noalloc(int64_t n, int32_t max_delay, void *state_dev, const float *vtmp_dev, const uint16_t *cls_dev,
+                     const bsim_class_params *ctab_dev, const int64_t *row_off_dev, const uint32_t *syn_dev,
+                     int32_t *fire_count_dev, int64_t steps, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
