@@ -3,8 +3,8 @@
 // One launch advances every network in the engine by one cycle. Its blocks
 // first run the LIF_brian update over a grid-stride share of the neurons
 // (reads the synaptic input summed during the previous launch, writes the new
-// state, appends fired ids to this cycle's ring slot with one atomic per warp
-// and stores the warp's ballot as a fired-bitmap word), then deliver the
+// state, appends fired ids to this cycle's ring slot with one atomic per block
+// pass and stores each warp's ballot as a fired-bitmap word), then deliver the
 // spikes of cycles t-1 .. t-D into the input buffer of cycle t+1.
 //
 // The two halves touch disjoint data (the input accumulators are double
@@ -43,15 +43,21 @@ static __device__ __forceinline__ void red_add_u64(unsigned long long *p, unsign
 // sum rounded on its own (no FMA contraction), as the reference's x86 build
 // evaluates it:  v = ((Cm*v + v_tmp) + i_E*C_E) + i_I*C_I.
 // ---------------------------------------------------------------------------
+// Fired ids are appended to the cycle's ring slot with one global atomic per
+// block and pass: warps publish their ballot counts, warp 0 scans them and
+// reserves the block's range (a single counter per cycle would otherwise take
+// one same-address atomic per warp).
 template <int ACC>
-static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned long long t, int p, int cur)
+static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned long long t, int p, int cur,
+                                                 int *s_wcnt)
 {
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int32_t *slot_ids = a.ring + (int64_t)cur * a.cap;
     uint32_t *bm = a.bitmap + (int64_t)cur * a.W;
     int32_t *hist = a.pop_hist ? a.pop_hist + (int64_t)(t % (unsigned long long)a.hist_len) * a.n_pops : nullptr;
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < a.N; base += stride) {
+    for (int64_t bbase = (int64_t)blockIdx.x * blockDim.x; bbase < a.N; bbase += stride) {
+        const int64_t base = bbase + (threadIdx.x & ~31);
         const int64_t j = base + lane;
         bool fired = false;
         int pop = -1;
@@ -97,14 +103,27 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
             if (hist) pop = __ldg(&c->pop);
         }
         const unsigned mask = __ballot_sync(0xffffffffu, fired);
-        if (lane == 0) bm[base >> 5] = mask;
-        if (mask) {
-            const int leader = __ffs(mask) - 1;
+        if (lane == 0 && base < a.N) bm[base >> 5] = mask;
+        if (lane == 0) s_wcnt[warp] = __popc(mask);
+        __syncthreads();
+        if (warp == 0) {
+            int c = lane < nwarps ? s_wcnt[lane] : 0;
+            const int own = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int nb = __shfl_up_sync(0xffffffffu, c, o);
+                if (lane >= o) c += nb;
+            }
+            const int total = __shfl_sync(0xffffffffu, c, 31);
             int at = 0;
-            if (lane == leader) at = atomicAdd(&a.ring_cnt[cur], __popc(mask));
-            at = __shfl_sync(0xffffffffu, at, leader);
+            if (lane == 0 && total) at = atomicAdd(&a.ring_cnt[cur], total);
+            at = __shfl_sync(0xffffffffu, at, 0);
+            if (lane < nwarps) s_wcnt[32 + lane] = at + c - own;  // this warp's first position
+        }
+        __syncthreads();
+        if (mask) {
             if (fired) {
-                slot_ids[at + __popc(mask & ((1u << lane) - 1u))] = (int32_t)j;
+                slot_ids[s_wcnt[32 + warp] + __popc(mask & ((1u << lane) - 1u))] = (int32_t)j;
                 a.fire_count[j] += 1;
             }
             if (hist) {
@@ -113,6 +132,7 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
                 if (fired && lane == __ffs(same) - 1) atomicAdd(&hist[pop], __popc(same));
             }
         }
+        __syncthreads();  // s_wcnt is reused by the next pass
     }
 }
 
@@ -129,7 +149,13 @@ static __device__ __forceinline__ void push_one(unsigned long long *acc, uint32_
 }
 
 // (spike, delay) segments whose metadata one warp resolves at once
+#ifndef PUSH_CHUNK
 #define PUSH_CHUNK 8
+#endif
+// resident blocks of 512 threads the step kernel is compiled for
+#ifndef STEP_MIN_BLOCKS
+#define STEP_MIN_BLOCKS 1
+#endif
 #define MAX_WARPS 16
 
 struct PushSeg {
@@ -345,10 +371,11 @@ static __device__ __forceinline__ void record_phase(const StepArgs &a, unsigned 
 }
 
 template <int ACC>
-__global__ void __launch_bounds__(512) step_kernel(const StepArgs a)
+__global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const StepArgs a)
 {
     __shared__ long long s_cum[BSIM_MAX_DELAY + 1];
     __shared__ PushSeg s_seg[MAX_WARPS * PUSH_CHUNK];
+    __shared__ int s_wcnt[64];
     __shared__ unsigned long long s_ev;
     const unsigned long long t = *reinterpret_cast<volatile unsigned long long *>(a.step_ctr);
     const int p = (int)(t & 1ull);
@@ -365,7 +392,7 @@ __global__ void __launch_bounds__(512) step_kernel(const StepArgs a)
         int32_t *nxt = a.pop_hist + (int64_t)((t + 1) % (unsigned long long)a.hist_len) * a.n_pops;
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_pops; i += gridDim.x * blockDim.x) nxt[i] = 0;
     }
-    lif_phase<ACC>(a, t, p, cur);
+    lif_phase<ACC>(a, t, p, cur, s_wcnt);
     record_phase(a, t);
     __syncthreads();  // publishes s_cum and s_ev
     unsigned long long ev;
