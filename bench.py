@@ -215,7 +215,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=200)
     ap.add_argument("--config", default="plain_1m")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--delivery", default="push", choices=["push", "pull"])
+    ap.add_argument("--delivery", default="push", choices=["push", "pull", "tile", "auto"])
     ap.add_argument("--settle", type=int, default=1000,
                     help="untimed cycles run at set-up so the network leaves its start-up transient")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -239,7 +239,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
     specs, desc = workload(args.config, 1 + rank)
-    deliv = B.DELIVERY_PULL if args.delivery == "pull" else B.DELIVERY_PUSH
+    deliv = {"push": B.DELIVERY_PUSH, "pull": B.DELIVERY_PULL, "tile": B.DELIVERY_TILE,
+             "auto": B.DELIVERY_AUTO}[args.delivery]
     t_build = time.perf_counter()
     eng = B.Engine.generated(specs, DT, opts=B.options(device=local, delivery=deliv, graph_steps=100))
     t_build = time.perf_counter() - t_build

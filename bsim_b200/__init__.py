@@ -22,6 +22,7 @@ ACC_ORDERED = 1
 DELIVERY_PUSH = 0
 DELIVERY_PULL = 1
 DELIVERY_AUTO = 2
+DELIVERY_TILE = 3
 MAX_DELAY = 1024
 
 
@@ -35,7 +36,8 @@ class Options(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("accumulate", ctypes.c_int32), ("delivery", ctypes.c_int32),
                 ("build_pull", ctypes.c_int32), ("graph_steps", ctypes.c_int32),
                 ("block_threads", ctypes.c_int32), ("grid_blocks", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 9)]
+                ("build_tiles", ctypes.c_int32), ("tile_size", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 7)]
 
 
 class GenSpec(ctypes.Structure):

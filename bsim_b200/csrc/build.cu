@@ -23,6 +23,9 @@ namespace bsim {
 cudaError_t launch_step(Engine &e);
 cudaError_t launch_record_flush(Engine &e);
 cudaError_t step_occupancy(int block, int accumulate, int *blocks_per_sm);
+cudaError_t step_occupancy(int block, int accumulate, int *blocks_per_sm, size_t smem);
+size_t step_dynamic_smem(const StepArgs &a);
+cudaError_t step_set_smem(int accumulate, size_t bytes);
 
 static thread_local std::string g_err;
 
@@ -126,6 +129,9 @@ static uint32_t f2u(float f)
 }
 
 static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab);
+static bool wants_tiles(const bsim_options &o, int32_t D);
+static int build_tiles_host(Engine &e, const int32_t *inst, const int32_t *src, const int32_t *dst,
+                            const float *weight, const int32_t *delay, int64_t s);
 
 static int init_device(Engine &e, const bsim_options *opt)
 {
@@ -136,7 +142,9 @@ static int init_device(Engine &e, const bsim_options *opt)
     CK(cudaDeviceGetAttribute(&e.sm_count, cudaDevAttrMultiProcessorCount, e.device));
     CK(cudaStreamCreateWithFlags(&e.stream, cudaStreamNonBlocking));
     if (e.opt.accumulate == BSIM_ACC_ORDERED) e.opt.delivery = BSIM_DELIVERY_PULL;
-    if (e.opt.accumulate == BSIM_ACC_ORDERED || e.opt.delivery != BSIM_DELIVERY_PUSH) e.opt.build_pull = 1;
+    if (e.opt.accumulate == BSIM_ACC_ORDERED || e.opt.delivery == BSIM_DELIVERY_PULL) e.opt.build_pull = 1;
+    if (e.opt.accumulate == BSIM_ACC_ORDERED && e.opt.delivery == BSIM_DELIVERY_TILE)
+        return fail(BSIM_ERR_ARG, "tiled delivery needs EXACT accumulation");
     return BSIM_OK;
 }
 
@@ -326,6 +334,13 @@ static int create_from_arrays(const float *params, int64_t n, const int32_t *pop
         free_engine(e);
         return fail(BSIM_ERR_CUDA, std::string("bsim_create upload: ") + cudaGetErrorString(st));
     }
+    if (wants_tiles(e->opt, D)) {
+        rc = build_tiles_host(*e, inst, src, dst, weight, delay, s);
+        if (rc != BSIM_OK) {
+            free_engine(e);
+            return rc;
+        }
+    }
     rc = finish_engine(*e, ctab);
     if (rc != BSIM_OK) {
         free_engine(e);
@@ -383,16 +398,171 @@ static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
     a.pop_hist = nullptr;
     a.n_pops = e.n_pops;
     a.hist_len = 0;
-    // launch shape: enough resident warps to cover HBM latency, at most one
-    // thread per neuron-group of work for small networks
+    a.fire_hist = nullptr;
+    if (a.n_tiles > 0) {
+        unsigned long long *d_hist;
+        TRY(dalloc(e, &d_hist, 2 * (size_t)e.N));
+        CK(cudaMemset(d_hist, 0, sizeof(unsigned long long) * 2 * (size_t)e.N));
+        a.fire_hist = d_hist;
+        if (e.opt.delivery == BSIM_DELIVERY_TILE) a.delivery = BSIM_DELIVERY_TILE;
+    }
+    // launch shape: all blocks resident (occupancy-sized grid), so the grid-stride
+    // loops of both phases see every SM
     e.block = e.opt.block_threads > 0 ? e.opt.block_threads : 512;
     if (e.block % 32 != 0 || e.block > 512) return fail(BSIM_ERR_ARG, "block_threads must be a multiple of 32 <= 512");
+    const size_t smem = step_dynamic_smem(a);
+    if (smem > 0) CK(step_set_smem(e.opt.accumulate, smem));
     int bps = 0;
-    CK(step_occupancy(e.block, e.opt.accumulate, &bps));
-    if (bps < 1) bps = 1;
+    CK(step_occupancy(e.block, e.opt.accumulate, &bps, smem));
+    if (bps < 1) return fail(BSIM_ERR_LIMIT, "step kernel does not fit on an SM with this tile size");
     e.grid = e.opt.grid_blocks > 0 ? e.opt.grid_blocks : e.sm_count * bps;
     CK(cudaDeviceSynchronize());
     return BSIM_OK;
+}
+
+// Target tiles: contiguous neuron ranges that never straddle two networks, of
+// near-equal size <= tile (so one shared-memory accumulator array fits them).
+static int plan_tiles(const std::vector<int64_t> &run_beg, int64_t tile, std::vector<int32_t> &tile_beg,
+                      int32_t &tile_max)
+{
+    tile_beg.clear();
+    tile_max = 0;
+    for (size_t r = 0; r + 1 < run_beg.size(); r++) {
+        const int64_t b = run_beg[r], len = run_beg[r + 1] - b;
+        if (len <= 0) continue;
+        const int64_t k = (len + tile - 1) / tile;
+        for (int64_t i = 0; i < k; i++) {
+            const int64_t s0 = b + len * i / k, s1 = b + len * (i + 1) / k;
+            tile_beg.push_back((int32_t)s0);
+            tile_max = std::max<int32_t>(tile_max, (int32_t)(s1 - s0));
+        }
+    }
+    tile_beg.push_back((int32_t)run_beg.back());
+    return BSIM_OK;
+}
+
+static int64_t auto_tile_size(const bsim_options &o, int64_t N, int sm_count)
+{
+    if (o.tile_size > 0) return std::min<int64_t>(o.tile_size, 8192);
+    int64_t t = (N + 2 * sm_count - 1) / (2 * sm_count);
+    return std::max<int64_t>(256, std::min<int64_t>(8192, t));
+}
+
+static bool wants_tiles(const bsim_options &o, int32_t D)
+{
+    return o.accumulate == BSIM_ACC_EXACT && D <= 64 &&
+           (o.build_tiles || o.delivery == BSIM_DELIVERY_TILE || o.delivery == BSIM_DELIVERY_AUTO);
+}
+
+// Uploads the tile arrays and points the step arguments at them.
+static int upload_tiles(Engine &e, const std::vector<int32_t> &tile_beg, int32_t tile_max,
+                        const std::vector<float> &tile_scale, const std::vector<int64_t> &tile_pair_off,
+                        const std::vector<uint32_t> &pair_src, const std::vector<int64_t> &pair_base,
+                        const std::vector<uint16_t> &pair_doff, const std::vector<uint16_t> &ent_tgt,
+                        const std::vector<float> &ent_w)
+{
+    StepArgs &a = e.a;
+    const int32_t nt = (int32_t)tile_scale.size();
+    int32_t *d_tb;
+    float *d_ts, *d_ew;
+    int64_t *d_tpo, *d_pb;
+    uint32_t *d_ps;
+    uint16_t *d_pd, *d_et;
+    TRY(dalloc(e, &d_tb, nt + 1));
+    TRY(dalloc(e, &d_ts, nt));
+    TRY(dalloc(e, &d_tpo, nt + 1));
+    TRY(dalloc(e, &d_ps, pair_src.size()));
+    TRY(dalloc(e, &d_pb, pair_base.size()));
+    TRY(dalloc(e, &d_pd, pair_doff.size()));
+    TRY(dalloc(e, &d_et, ent_tgt.size()));
+    TRY(dalloc(e, &d_ew, ent_w.size()));
+    CK(cudaMemcpy(d_tb, tile_beg.data(), 4 * (nt + 1), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_ts, tile_scale.data(), 4 * nt, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_tpo, tile_pair_off.data(), 8 * (nt + 1), cudaMemcpyHostToDevice));
+    if (!pair_src.empty()) {
+        CK(cudaMemcpy(d_ps, pair_src.data(), 4 * pair_src.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d_pb, pair_base.data(), 8 * pair_base.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d_pd, pair_doff.data(), 2 * pair_doff.size(), cudaMemcpyHostToDevice));
+    }
+    if (!ent_tgt.empty()) {
+        CK(cudaMemcpy(d_et, ent_tgt.data(), 2 * ent_tgt.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d_ew, ent_w.data(), 4 * ent_w.size(), cudaMemcpyHostToDevice));
+    }
+    a.n_tiles = nt;
+    a.tile_max = tile_max;
+    a.tile_beg = d_tb;
+    a.tile_scale = d_ts;
+    a.tile_pair_off = d_tpo;
+    a.pair_src = d_ps;
+    a.pair_base = d_pb;
+    a.pair_doff = d_pd;
+    a.ent_tgt = d_et;
+    a.ent_w = d_ew;
+    return BSIM_OK;
+}
+
+// Host construction of the tiled copy: synapses sorted by (tile of target,
+// source, delay); one pair per distinct (tile, source).
+static int build_tiles_host(Engine &e, const int32_t *inst, const int32_t *src, const int32_t *dst,
+                            const float *weight, const int32_t *delay, int64_t s)
+{
+    const int64_t n = e.N;
+    const int32_t D = e.D;
+    std::vector<int64_t> runs = {0};
+    for (int64_t i = 1; i < n; i++)
+        if (inst && inst[i] != inst[i - 1]) runs.push_back(i);
+    runs.push_back(n);
+    std::vector<int32_t> tile_beg;
+    int32_t tile_max = 0;
+    plan_tiles(runs, auto_tile_size(e.opt, n, e.sm_count), tile_beg, tile_max);
+    const int32_t nt = (int32_t)tile_beg.size() - 1;
+    std::vector<int32_t> tile_of(n);
+    for (int32_t q = 0; q < nt; q++)
+        for (int64_t i = tile_beg[q]; i < tile_beg[q + 1]; i++) tile_of[i] = q;
+    std::vector<std::pair<uint64_t, int64_t>> key(s);
+    for (int64_t k = 0; k < s; k++)
+        key[k] = {((uint64_t)tile_of[dst[k]] << 37) | ((uint64_t)src[k] << 6) | (uint64_t)(delay[k] - 1), k};
+    std::sort(key.begin(), key.end());
+    std::vector<float> tile_scale(nt);
+    for (int32_t q = 0; q < nt; q++) tile_scale[q] = ldexpf(1.0f, e.qexp[inst ? inst[tile_beg[q]] : 0]);
+    std::vector<int64_t> tile_pair_off(nt + 1, 0);
+    std::vector<uint32_t> pair_src;
+    std::vector<int64_t> pair_base;
+    std::vector<uint16_t> pair_doff;
+    std::vector<uint16_t> ent_tgt(s);
+    std::vector<float> ent_w(s);
+    int64_t cur_pair_key = -1;
+    std::vector<int64_t> cnt(D + 1);
+    auto close_pair = [&]() -> bool {
+        if (cur_pair_key < 0) return true;
+        int64_t c = 0;
+        for (int d = 0; d <= D; d++) {
+            if (d > 0) c += cnt[d - 1];
+            if (c > 65535) return false;
+            pair_doff.push_back((uint16_t)c);
+        }
+        return true;
+    };
+    for (int64_t pos = 0; pos < s; pos++) {
+        const int64_t k = key[pos].second;
+        const int64_t pk = (int64_t)(key[pos].first >> 6);
+        const int32_t q = tile_of[dst[k]];
+        if (pk != cur_pair_key) {
+            if (!close_pair()) return fail(BSIM_ERR_LIMIT, "tiled delivery: more than 65535 synapses of one source into one tile");
+            std::fill(cnt.begin(), cnt.end(), 0);
+            cur_pair_key = pk;
+            pair_src.push_back((uint32_t)src[k]);
+            pair_base.push_back(pos);
+            tile_pair_off[q + 1] = (int64_t)pair_src.size();
+        }
+        cnt[delay[k] - 1]++;
+        ent_tgt[pos] = (uint16_t)(dst[k] - tile_beg[q]);
+        ent_w[pos] = weight[k];
+    }
+    if (!close_pair()) return fail(BSIM_ERR_LIMIT, "tiled delivery: more than 65535 synapses of one source into one tile");
+    for (int32_t q = 0; q < nt; q++) tile_pair_off[q + 1] = std::max(tile_pair_off[q + 1], tile_pair_off[q]);
+    return upload_tiles(e, tile_beg, tile_max, tile_scale, tile_pair_off, pair_src, pair_base, pair_doff, ent_tgt,
+                        ent_w);
 }
 
 // ---------------------------------------------------------------------------
@@ -560,6 +730,83 @@ __global__ void gen_pull_kernel(GenDev g, int64_t N, int64_t *col_cnt_or_off, ui
     }
 }
 
+// One (tile, incoming projection) piece of the tiled copy: the sources of the
+// projection's population against the targets [j0, j1) of its target
+// population that lie in the tile. Its pairs are pair_start + source index.
+struct TileSeg {
+    int64_t pair_start;
+    uint64_t pseed;
+    int64_t src_base;   // global id of source 0
+    int32_t j0, j1;     // target range, local to the target population
+    int32_t tgt_off;    // offset of target j0 inside the tile
+    int32_t n_src;
+    uint32_t p24, exc24;
+    float w_exc, w_inh;
+    int32_t d_inst;     // the network's max delay
+    int32_t pad;
+};
+
+static __device__ __forceinline__ int find_seg(const TileSeg *segs, int n_segs, int64_t k)
+{
+    int lo = 0, hi = n_segs - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (segs[mid].pair_start <= k) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// One warp per (tile, source) pair. Pass 0: per-delay counts -> cumulative
+// pair_doff and pair_cnt. Pass 1: entries in delay order, targets ascending.
+template <int PASS>
+__global__ void gen_tile_kernel(const TileSeg *segs, int n_segs, int64_t n_pairs, int D, uint32_t *pair_src,
+                                int64_t *pair_cnt, uint16_t *pair_doff, const int64_t *pair_base,
+                                uint16_t *ent_tgt, float *ent_w)
+{
+    __shared__ long long s_cur[8][GEN_MAX_DELAY];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    long long *cur = s_cur[wib];
+    for (int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < n_pairs;
+         k += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const TileSeg sg = segs[find_seg(segs, n_segs, k)];
+        const int64_t i = k - sg.pair_start;
+        uint16_t *doff = pair_doff + k * (D + 1);
+        for (int d = lane; d < D; d += 32) cur[d] = PASS == 0 ? 0 : pair_base[k] + doff[d];
+        __syncwarp();
+        for (int j0 = sg.j0; j0 < sg.j1; j0 += 32) {
+            const int j = j0 + lane;
+            SynDraw sd;
+            const bool conn = j < sg.j1 && draw_pair(sg.pseed, (uint64_t)i, (uint64_t)j, sg.p24, sg.exc24, sg.w_exc,
+                                                     sg.w_inh, sg.d_inst, &sd);
+            if (!__ballot_sync(0xffffffffu, conn)) continue;
+            const unsigned same = __match_any_sync(0xffffffffu, conn ? sd.d : -1);
+            if (conn) {
+                const int leader = __ffs(same) - 1;
+                const long long at = cur[sd.d - 1] + __popc(same & ((1u << lane) - 1u));
+                if (PASS == 1) {
+                    ent_tgt[at] = (uint16_t)(sg.tgt_off + (j - sg.j0));
+                    ent_w[at] = sd.w;
+                }
+                __syncwarp(same);
+                if (lane == leader) cur[sd.d - 1] += __popc(same);
+            }
+            __syncwarp();
+        }
+        __syncwarp();
+        if (PASS == 0 && lane == 0) {
+            long long c = 0;
+            for (int d = 0; d <= D; d++) {
+                doff[d] = (uint16_t)c;
+                if (d < D) c += cur[d];
+            }
+            pair_cnt[k] = c;
+            pair_src[k] = (uint32_t)(sg.src_base + i);
+        }
+        __syncwarp();
+    }
+}
+
 // Remote projection choice of one generated network (host side, shared by
 // the host generator and the device builder).
 struct GenPlan {
@@ -621,10 +868,12 @@ static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, co
     int32_t D = 1, n_cls = 0;
     std::vector<ClassParams> ctab;
     std::vector<float> cls_rm, cls_Cm;
+    std::vector<GenPlan> plans(ns);
     for (int k = 0; k < ns; k++) {
         const bsim_gen_spec &g = specs[k];
         TRY(check_spec(g));
-        GenPlan pl = gen_plan(g);
+        plans[k] = gen_plan(g);
+        const GenPlan &pl = plans[k];
         GenInst &x = gi[k];
         x.nbase = N;
         x.P = g.n_pop;
@@ -758,13 +1007,103 @@ static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, co
         E.a.csc_w = d_cw;
         E.a.csc_d = d_cd;
     }
-    // push rows
-    const int64_t nrows = N * (int64_t)D;
-    int64_t *d_row; uint2 *d_syn;
-    if ((rc = dalloc(E, &d_row, nrows + 1)) || (rc = dalloc(E, &d_syn, S))) { free_tmp(); return bail(rc); }
-    gen_push_kernel<0><<<gb, 256, 0, E.stream>>>(gd, N, d_row, nullptr);
-    if ((rc = scan(d_row, nrows))) { free_tmp(); return bail(rc); }
-    gen_push_kernel<1><<<gb, 256, 0, E.stream>>>(gd, N, d_row, d_syn);
+    // target-tiled copy
+    const bool tiles = wants_tiles(E.opt, D);
+    if (tiles) {
+        std::vector<int64_t> runs;
+        for (int k = 0; k < ns; k++) runs.push_back(gi[k].nbase);
+        runs.push_back(N);
+        std::vector<int32_t> tile_beg;
+        int32_t tile_max = 0;
+        plan_tiles(runs, auto_tile_size(E.opt, N, E.sm_count), tile_beg, tile_max);
+        const int32_t nt = (int32_t)tile_beg.size() - 1;
+        std::vector<TileSeg> segs;
+        std::vector<int64_t> tile_pair_off(nt + 1);
+        std::vector<float> tile_scale(nt);
+        int64_t pairs = 0;
+        int k = 0;
+        for (int32_t q = 0; q < nt; q++) {
+            while (k + 1 < ns && gi[k + 1].nbase <= tile_beg[q]) k++;
+            const GenInst &x = gi[k];
+            const GenPlan &pl = plans[k];
+            tile_pair_off[q] = pairs;
+            tile_scale[q] = ldexpf(1.0f, E.qexp[k]);
+            const int64_t lb = tile_beg[q] - x.nbase, le = tile_beg[q + 1] - x.nbase;
+            for (int64_t pp = lb / x.n; pp <= (le - 1) / x.n; pp++) {
+                const int64_t pop_beg = pp * x.n;
+                const int32_t j0 = (int32_t)(std::max(lb, pop_beg) - pop_beg);
+                const int32_t j1 = (int32_t)(std::min(le, pop_beg + x.n) - pop_beg);
+                for (int id : pl.in[pp]) {
+                    TileSeg sg;
+                    sg.pair_start = pairs;
+                    sg.pseed = pl.proj[id].pseed;
+                    sg.src_base = x.nbase + (int64_t)pl.proj[id].src_pop * x.n;
+                    sg.j0 = j0;
+                    sg.j1 = j1;
+                    sg.tgt_off = (int32_t)(pop_beg + j0 - lb);
+                    sg.n_src = x.n;
+                    sg.p24 = x.p24;
+                    sg.exc24 = x.exc24;
+                    sg.w_exc = x.w_exc;
+                    sg.w_inh = x.w_inh;
+                    sg.d_inst = x.D;
+                    sg.pad = 0;
+                    segs.push_back(sg);
+                    pairs += x.n;
+                }
+            }
+        }
+        tile_pair_off[nt] = pairs;
+        TileSeg *d_segs;
+        int64_t *d_pcnt;
+        if ((rc = talloc((void **)&d_segs, sizeof(TileSeg) * std::max<size_t>(1, segs.size()))) ||
+            (rc = talloc((void **)&d_pcnt, sizeof(int64_t) * (pairs + 1)))) { free_tmp(); return bail(rc); }
+        if (!segs.empty()) cudaMemcpy(d_segs, segs.data(), sizeof(TileSeg) * segs.size(), cudaMemcpyHostToDevice);
+        int32_t *d_tb; float *d_ts, *d_ew; int64_t *d_tpo, *d_pb; uint32_t *d_ps; uint16_t *d_pd, *d_et;
+        if ((rc = dalloc(E, &d_tb, nt + 1)) || (rc = dalloc(E, &d_ts, nt)) || (rc = dalloc(E, &d_tpo, nt + 1)) ||
+            (rc = dalloc(E, &d_ps, pairs)) || (rc = dalloc(E, &d_pb, pairs + 1)) ||
+            (rc = dalloc(E, &d_pd, (size_t)pairs * (D + 1))) || (rc = dalloc(E, &d_et, S)) || (rc = dalloc(E, &d_ew, S))) {
+            free_tmp();
+            return bail(rc);
+        }
+        cudaMemcpy(d_tb, tile_beg.data(), 4 * (nt + 1), cudaMemcpyHostToDevice);
+        cudaMemcpy(d_ts, tile_scale.data(), 4 * nt, cudaMemcpyHostToDevice);
+        cudaMemcpy(d_tpo, tile_pair_off.data(), 8 * (nt + 1), cudaMemcpyHostToDevice);
+        gen_tile_kernel<0><<<gb, 256, 0, E.stream>>>(d_segs, (int)segs.size(), pairs, D, d_ps, d_pcnt, d_pd, nullptr,
+                                                    nullptr, nullptr);
+        cudaMemcpyAsync(d_pb, d_pcnt, sizeof(int64_t) * pairs, cudaMemcpyDeviceToDevice, E.stream);
+        if ((rc = scan(d_pb, pairs))) { free_tmp(); return bail(rc); }
+        gen_tile_kernel<1><<<gb, 256, 0, E.stream>>>(d_segs, (int)segs.size(), pairs, D, d_ps, d_pcnt, d_pd, d_pb,
+                                                    d_et, d_ew);
+        int64_t tot = -1;
+        cudaMemcpyAsync(&tot, d_pb + pairs, 8, cudaMemcpyDeviceToHost, E.stream);
+        if (cudaStreamSynchronize(E.stream) != cudaSuccess || tot != S) {
+            free_tmp();
+            return bail(fail(BSIM_ERR_CUDA, "generator: tiled copy does not match the synapse count"));
+        }
+        StepArgs &a = E.a;
+        a.n_tiles = nt;
+        a.tile_max = tile_max;
+        a.tile_beg = d_tb;
+        a.tile_scale = d_ts;
+        a.tile_pair_off = d_tpo;
+        a.pair_src = d_ps;
+        a.pair_base = d_pb;
+        a.pair_doff = d_pd;
+        a.ent_tgt = d_et;
+        a.ent_w = d_ew;
+    }
+    // push rows (not needed when every step uses the tiled copy)
+    if (!(tiles && E.opt.delivery == BSIM_DELIVERY_TILE)) {
+        const int64_t nrows = N * (int64_t)D;
+        int64_t *d_row; uint2 *d_syn;
+        if ((rc = dalloc(E, &d_row, nrows + 1)) || (rc = dalloc(E, &d_syn, S))) { free_tmp(); return bail(rc); }
+        gen_push_kernel<0><<<gb, 256, 0, E.stream>>>(gd, N, d_row, nullptr);
+        if ((rc = scan(d_row, nrows))) { free_tmp(); return bail(rc); }
+        gen_push_kernel<1><<<gb, 256, 0, E.stream>>>(gd, N, d_row, d_syn);
+        E.a.row_off = d_row;
+        E.a.syn = d_syn;
+    }
     cudaError_t st = cudaStreamSynchronize(E.stream);
     if (st == cudaSuccess) st = cudaGetLastError();
     free_tmp();
@@ -772,8 +1111,6 @@ static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, co
     E.a.state = d_state;
     E.a.vtmp = d_vtmp;
     E.a.cls = d_cls;
-    E.a.row_off = d_row;
-    E.a.syn = d_syn;
     rc = finish_engine(E, ctab);
     if (rc != BSIM_OK) return bail(rc);
     *out = e;

@@ -101,6 +101,11 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
             st.w = __int_as_float(refrac);
             a.state[j] = st;
             if (hist) pop = __ldg(&c->pop);
+            if (a.fire_hist) {
+                // per-neuron shift register of the last 64 cycles (tiled delivery's source filter)
+                const unsigned long long old = a.fire_hist[(int64_t)(p ^ 1) * a.N + j];
+                a.fire_hist[(int64_t)p * a.N + j] = (old << 1) | (fired ? 1ull : 0ull);
+            }
         }
         const unsigned mask = __ballot_sync(0xffffffffu, fired);
         if (lane == 0 && base < a.N) bm[base >> 5] = mask;
@@ -154,7 +159,7 @@ static __device__ __forceinline__ void push_one(unsigned long long *acc, uint32_
 #endif
 // resident blocks of 512 threads the step kernel is compiled for
 #ifndef STEP_MIN_BLOCKS
-#define STEP_MIN_BLOCKS 1
+#define STEP_MIN_BLOCKS 2
 #endif
 #define MAX_WARPS 16
 
@@ -344,6 +349,127 @@ static __device__ __forceinline__ unsigned long long pull_phase(const StepArgs &
     return lane == 0 ? ev : 0ull;
 }
 
+// ---------------------------------------------------------------------------
+// Phase B, tiled: each block owns a contiguous tile of target neurons and sums
+// their input exactly in shared memory (int64 fixed point), so no global atomic
+// is issued; the tile is written out once at the end. The tile's synapses are
+// grouped by (source, delay): a warp takes 32 (tile, source) pairs, filters them
+// with each source's fire history (bit d-1: fired d cycles ago), gathers the
+// active (pair, delay) segments into a per-warp list and streams their entries
+// ({u16 target offset, f32 weight}) as one flat range.
+// ---------------------------------------------------------------------------
+#define TILE_SEGS 64
+
+static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &a, int p, int pw,
+                                                                unsigned long long *s_acc, long long *s_start,
+                                                                int *s_cum)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int D = a.D;
+    const unsigned long long dmask = D >= 64 ? ~0ull : ((1ull << D) - 1ull);
+    long long *seg_start = s_start + warp * TILE_SEGS;
+    int *seg_cum = s_cum + warp * TILE_SEGS;
+    const unsigned long long *hist = a.fire_hist + (int64_t)(p ^ 1) * a.N;  // state after cycle t-1
+    unsigned long long ev = 0;
+    for (int q = blockIdx.x; q < a.n_tiles; q += gridDim.x) {
+        const int tb = a.tile_beg[q], T = a.tile_beg[q + 1] - tb;
+        for (int i = threadIdx.x; i < 2 * T; i += blockDim.x) s_acc[i] = 0ull;
+        __syncthreads();
+        const float sc = a.tile_scale[q];
+        const int64_t k0 = a.tile_pair_off[q], k1 = a.tile_pair_off[q + 1];
+        for (int64_t kb = k0 + (int64_t)warp * 32; kb < k1; kb += (int64_t)nwarps * 32) {
+            const int64_t k = kb + lane;
+            unsigned long long m = 0;
+            int64_t pbase = 0;
+            const uint16_t *doff = nullptr;
+            if (k < k1) {
+                m = hist[a.pair_src[k]] & dmask;
+                if (m) {
+                    pbase = a.pair_base[k];
+                    doff = a.pair_doff + k * (D + 1);
+                }
+            }
+            while (__any_sync(0xffffffffu, m != 0)) {
+                // this round: up to TILE_SEGS (pair, delay) segments of the warp
+                const int cnt = __popcll(m);
+                int incl = cnt;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int nb = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += nb;
+                }
+                const int excl = incl - cnt;
+                const int total = __shfl_sync(0xffffffffu, incl, 31);
+                const int take = max(0, min(cnt, TILE_SEGS - excl));
+                for (int i = 0; i < take; i++) {
+                    const int b = __ffsll((long long)m) - 1;
+                    m &= m - 1;
+                    const int e0 = doff[b], e1 = doff[b + 1];
+                    seg_start[excl + i] = pbase + e0;
+                    seg_cum[excl + i] = e1 - e0;  // length for now
+                }
+                __syncwarp();
+                const int nseg = min(total, TILE_SEGS);
+                // inclusive prefix of the segment lengths (two per lane)
+                int l0 = lane < nseg ? seg_cum[lane] : 0;
+                int l1 = lane + 32 < nseg ? seg_cum[lane + 32] : 0;
+                int c0 = l0, c1 = l1;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int n0 = __shfl_up_sync(0xffffffffu, c0, o);
+                    const int n1 = __shfl_up_sync(0xffffffffu, c1, o);
+                    if (lane >= o) {
+                        c0 += n0;
+                        c1 += n1;
+                    }
+                }
+                const int half = __shfl_sync(0xffffffffu, c0, 31);
+                __syncwarp();
+                if (lane < nseg) seg_cum[lane] = c0;
+                if (lane + 32 < nseg) seg_cum[lane + 32] = half + c1;
+                __syncwarp();
+                const int n_ent = seg_cum[nseg - 1];
+                if (lane == 0) ev += (unsigned long long)n_ent;
+                for (int f0 = 0; f0 < n_ent; f0 += 4 * 32) {
+                    uint16_t tg[4];
+                    float wv[4];
+                    bool ok[4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const int f = f0 + u * 32 + lane;
+                        ok[u] = f < n_ent;
+                        if (ok[u]) {
+                            int lo = 0, hi = nseg - 1;
+                            while (lo < hi) {
+                                const int mid = (lo + hi) >> 1;
+                                if (seg_cum[mid] > f) hi = mid;
+                                else lo = mid + 1;
+                            }
+                            const int64_t e = seg_start[lo] + (f - (lo ? seg_cum[lo - 1] : 0));
+                            tg[u] = __ldcs(a.ent_tgt + e);
+                            wv[u] = __ldcs(a.ent_w + e);
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        if (ok[u]) {
+                            const long long qv = __float2ll_rn(__fmul_rn(wv[u], sc));
+                            atomicAdd(s_acc + 2 * (int)tg[u] + (wv[u] >= 0.0f ? 0 : 1), (unsigned long long)qv);
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        longlong2 *g = reinterpret_cast<longlong2 *>(a.acc) + (int64_t)pw * a.N + tb;
+        for (int i = threadIdx.x; i < T; i += blockDim.x)
+            g[i] = make_longlong2((long long)s_acc[2 * i], (long long)s_acc[2 * i + 1]);
+        __syncthreads();
+    }
+    return ev;
+}
+
 // Copies the complete ring slot of cycle t-1 into the raster recording.
 static __device__ __forceinline__ void record_phase(const StepArgs &a, unsigned long long t)
 {
@@ -377,11 +503,15 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const StepAr
     __shared__ PushSeg s_seg[MAX_WARPS * PUSH_CHUNK];
     __shared__ int s_wcnt[64];
     __shared__ unsigned long long s_ev;
+    // tiled delivery: [2 * tile_max] u64 accumulators, then per-warp segment lists
+    extern __shared__ __align__(16) unsigned long long s_dyn[];
     const unsigned long long t = *reinterpret_cast<volatile unsigned long long *>(a.step_ctr);
     const int p = (int)(t & 1ull);
     const int cur = (int)(t % (unsigned long long)a.R);
-    const int dm = a.deliv_sel ? *a.deliv_sel : a.delivery;
-    const bool push = ACC != BSIM_ACC_ORDERED && dm != BSIM_DELIVERY_PULL;
+    int dm = a.deliv_sel ? *a.deliv_sel : a.delivery;
+    if (dm == BSIM_DELIVERY_TILE && a.n_tiles == 0) dm = BSIM_DELIVERY_PUSH;
+    const bool push = ACC != BSIM_ACC_ORDERED && dm == BSIM_DELIVERY_PUSH;
+    const bool tiled = ACC != BSIM_ACC_ORDERED && dm == BSIM_DELIVERY_TILE;
     if (threadIdx.x == 0) s_ev = 0;
     if (push && threadIdx.x < 32) delay_window_prefix(a, t, s_cum);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -396,8 +526,15 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const StepAr
     record_phase(a, t);
     __syncthreads();  // publishes s_cum and s_ev
     unsigned long long ev;
-    if (push) ev = push_phase(a, t, p ^ 1, s_cum, s_seg);
-    else ev = pull_phase<ACC>(a, t, p ^ 1);
+    if (push) {
+        ev = push_phase(a, t, p ^ 1, s_cum, s_seg);
+    } else if (tiled) {
+        long long *starts = reinterpret_cast<long long *>(s_dyn + 2 * a.tile_max);
+        int *cums = reinterpret_cast<int *>(starts + MAX_WARPS * TILE_SEGS);
+        ev = tile_phase(a, p, p ^ 1, s_dyn, starts, cums);
+    } else {
+        ev = pull_phase<ACC>(a, t, p ^ 1);
+    }
     if (ev) atomicAdd(&s_ev, ev);
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -446,12 +583,42 @@ __global__ void record_flush_kernel(const StepArgs a)
     }
 }
 
+// Dynamic shared memory of the step kernel: the tile accumulators and the
+// per-warp segment lists of tiled delivery (0 when no tiles are built).
+size_t step_dynamic_smem(const StepArgs &a)
+{
+    if (a.n_tiles == 0) return 0;
+    return (size_t)2 * a.tile_max * sizeof(unsigned long long) +
+           (size_t)MAX_WARPS * TILE_SEGS * (sizeof(long long) + sizeof(int));
+}
+
+// The attribute belongs to the kernel, not to an engine: it only ever grows,
+// so an engine built later with smaller tiles cannot break an earlier one.
+cudaError_t step_set_smem(int accumulate, size_t bytes)
+{
+    static size_t set_bytes[64][2];
+    int dev = 0;
+    cudaError_t st = cudaGetDevice(&dev);
+    if (st != cudaSuccess) return st;
+    const int k = accumulate == BSIM_ACC_ORDERED ? 1 : 0;
+    if (dev < 0 || dev >= 64 || bytes <= set_bytes[dev][k]) return cudaSuccess;
+    if (accumulate == BSIM_ACC_ORDERED)
+        st = cudaFuncSetAttribute(step_kernel<BSIM_ACC_ORDERED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)bytes);
+    else
+        st = cudaFuncSetAttribute(step_kernel<BSIM_ACC_EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)bytes);
+    if (st == cudaSuccess) set_bytes[dev][k] = bytes;
+    return st;
+}
+
 cudaError_t launch_step(Engine &e)
 {
+    const size_t smem = step_dynamic_smem(e.a);
     if (e.opt.accumulate == BSIM_ACC_ORDERED)
-        step_kernel<BSIM_ACC_ORDERED><<<e.grid, e.block, 0, e.stream>>>(e.a);
+        step_kernel<BSIM_ACC_ORDERED><<<e.grid, e.block, smem, e.stream>>>(e.a);
     else
-        step_kernel<BSIM_ACC_EXACT><<<e.grid, e.block, 0, e.stream>>>(e.a);
+        step_kernel<BSIM_ACC_EXACT><<<e.grid, e.block, smem, e.stream>>>(e.a);
     return cudaGetLastError();
 }
 
@@ -468,11 +635,17 @@ cudaError_t launch_record_flush(Engine &e)
     return cudaGetLastError();
 }
 
-cudaError_t step_occupancy(int block, int accumulate, int *blocks_per_sm)
+cudaError_t step_occupancy(int block, int accumulate, int *blocks_per_sm, size_t smem)
 {
     if (accumulate == BSIM_ACC_ORDERED)
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<BSIM_ACC_ORDERED>, block, 0);
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<BSIM_ACC_EXACT>, block, 0);
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<BSIM_ACC_ORDERED>, block,
+                                                             smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<BSIM_ACC_EXACT>, block, smem);
+}
+
+cudaError_t step_occupancy(int block, int accumulate, int *blocks_per_sm)
+{
+    return step_occupancy(block, accumulate, blocks_per_sm, 0);
 }
 
 }  // namespace bsim

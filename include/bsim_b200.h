@@ -47,6 +47,8 @@ extern "C" {
 #define BSIM_DELIVERY_PUSH 0 /* source-ordered rows, one warp per (spike, delay) segment */
 #define BSIM_DELIVERY_PULL 1 /* target-ordered rows scanned against per-step fired bitmaps */
 #define BSIM_DELIVERY_AUTO 2 /* per step, by the firing predictor (EXACT accumulation only) */
+#define BSIM_DELIVERY_TILE 3 /* target tiles summed in shared memory, sources filtered by their
+                                fire history (EXACT accumulation only; delays up to 64) */
 
 typedef struct bsim_engine bsim_engine;
 
@@ -58,7 +60,9 @@ typedef struct bsim_options {
     int32_t graph_steps;   /* steps captured per CUDA graph by bsim_run (0: plain launches) */
     int32_t block_threads; /* threads per block of the step kernel (0: autotuned) */
     int32_t grid_blocks;   /* blocks of the step kernel (0: autotuned) */
-    int32_t reserved[9];
+    int32_t build_tiles;   /* also build the target-tiled copy (forced on for TILE/AUTO) */
+    int32_t tile_size;     /* target neurons per tile (0: chosen from the network size, <= 8192) */
+    int32_t reserved[7];
 } bsim_options;
 
 /* Parameters of one generated network (see bsim_create_generated). */

@@ -198,3 +198,33 @@ def test_scaled_replicas_vs_oracle(name, spec, steps):
     assert same_raster(raster, fx["raster"]) is None
     assert np.array_equal(vs[-1], fx["v_trace"][-1])
     assert eng.info().events_total == fx["events_per_step"].sum()
+
+
+@pytest.mark.parametrize("opts", [dict(), dict(tile_size=300), dict(tile_size=256, block_threads=256)])
+def test_tiled_delivery_identical_to_push(c0, opts):
+    """Target-tiled delivery (shared-memory sums) equals push delivery bit for bit,
+    device-built and host-built, including tiles that straddle populations."""
+    spec, g = c0
+    ref = B.Engine.generated(spec, DT)
+    r_ref, v_ref = run_checkpoints(ref, 400, 400)
+    for eng in (B.Engine.generated(spec, DT, opts=B.options(delivery=B.DELIVERY_TILE, **opts)),
+                engine_from(g, delivery=B.DELIVERY_TILE, **opts)):
+        r, v = run_checkpoints(eng, 400, 400)
+        assert same_raster(r, r_ref) is None
+        assert np.array_equal(v[-1], v_ref[-1])
+        assert eng.info().events_total == ref.info().events_total
+
+
+def test_tiled_batched_long_delays_equal_alone():
+    specs = [W.cuba(6, 700, 2000, 50, seed=41), W.cuba(5, 900, 100, 6, seed=42)]
+    both = B.Engine.generated(specs, DT, opts=B.options(delivery=B.DELIVERY_TILE, tile_size=512))
+    rb, _ = run_checkpoints(both, 300, 300)
+    base = 0
+    for sp in specs:
+        n = sp.n_pop * sp.pop_size
+        alone = B.Engine.generated(sp, DT)
+        ra, _ = run_checkpoints(alone, 300, 300)
+        for t in range(300):
+            mine = rb[t][(rb[t] >= base) & (rb[t] < base + n)] - base
+            assert np.array_equal(mine, ra[t]), t
+        base += n
