@@ -398,14 +398,7 @@ static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
     a.pop_hist = nullptr;
     a.n_pops = e.n_pops;
     a.hist_len = 0;
-    a.fire_hist = nullptr;
-    if (a.n_tiles > 0) {
-        unsigned long long *d_hist;
-        TRY(dalloc(e, &d_hist, 2 * (size_t)e.N));
-        CK(cudaMemset(d_hist, 0, sizeof(unsigned long long) * 2 * (size_t)e.N));
-        a.fire_hist = d_hist;
-        if (e.opt.delivery == BSIM_DELIVERY_TILE) a.delivery = BSIM_DELIVERY_TILE;
-    }
+    if (a.n_tiles > 0 && e.opt.delivery == BSIM_DELIVERY_TILE) a.delivery = BSIM_DELIVERY_TILE;
     // launch shape: all blocks resident (occupancy-sized grid), so the grid-stride
     // loops of both phases see every SM
     e.block = e.opt.block_threads > 0 ? e.opt.block_threads : 512;
@@ -441,11 +434,13 @@ static int plan_tiles(const std::vector<int64_t> &run_beg, int64_t tile, std::ve
     return BSIM_OK;
 }
 
+// 32 bytes of shared counters per target: tiles of <= 2048 targets let two
+// 512-thread blocks share an SM.
 static int64_t auto_tile_size(const bsim_options &o, int64_t N, int sm_count)
 {
-    if (o.tile_size > 0) return std::min<int64_t>(o.tile_size, 8192);
+    if (o.tile_size > 0) return std::min<int64_t>(o.tile_size, 4096);
     int64_t t = (N + 2 * sm_count - 1) / (2 * sm_count);
-    return std::max<int64_t>(256, std::min<int64_t>(8192, t));
+    return std::max<int64_t>(256, std::min<int64_t>(2048, t));
 }
 
 static bool wants_tiles(const bsim_options &o, int32_t D)
@@ -454,115 +449,168 @@ static bool wants_tiles(const bsim_options &o, int32_t D)
            (o.build_tiles || o.delivery == BSIM_DELIVERY_TILE || o.delivery == BSIM_DELIVERY_AUTO);
 }
 
-// Uploads the tile arrays and points the step arguments at them.
-static int upload_tiles(Engine &e, const std::vector<int32_t> &tile_beg, int32_t tile_max,
-                        const std::vector<float> &tile_scale, const std::vector<int64_t> &tile_pair_off,
-                        const std::vector<uint32_t> &pair_src, const std::vector<int64_t> &pair_base,
-                        const std::vector<uint16_t> &pair_doff, const std::vector<uint16_t> &ent_tgt,
-                        const std::vector<float> &ent_w)
+// Host-side description of the tiled copy.
+struct TileHost {
+    std::vector<int32_t> tile_beg, tile_run_off, tile_units, run_n, run_unit0;
+    std::vector<float> tile_scale;
+    std::vector<uint32_t> run_src0;
+    std::vector<int64_t> run_pair0;
+    int32_t tile_max = 0;
+};
+
+// Appends a run of sources [src0, src0 + n) to tile q (the last tile so far).
+static void add_run(TileHost &th, uint32_t src0, int32_t n, int64_t pair0, int32_t D)
+{
+    const int32_t q = (int32_t)th.tile_units.size() - 1;
+    th.run_src0.push_back(src0);
+    th.run_n.push_back(n);
+    th.run_pair0.push_back(pair0);
+    th.run_unit0.push_back(th.tile_units[q]);
+    th.tile_units[q] += ((n + 31) / 32) * D;
+    th.tile_run_off[q + 1] = (int32_t)th.run_src0.size();
+}
+
+// Uploads the tile tables (pair and entry arrays are uploaded by the caller)
+// and points the step arguments at them.
+static int upload_tiles(Engine &e, const TileHost &th)
 {
     StepArgs &a = e.a;
-    const int32_t nt = (int32_t)tile_scale.size();
-    int32_t *d_tb;
-    float *d_ts, *d_ew;
-    int64_t *d_tpo, *d_pb;
-    uint32_t *d_ps;
-    uint16_t *d_pd, *d_et;
+    const int32_t nt = (int32_t)th.tile_scale.size();
+    const size_t nr = th.run_src0.size();
+    int32_t *d_tb, *d_tro, *d_tu, *d_rn, *d_ru;
+    float *d_ts;
+    uint32_t *d_rs;
+    int64_t *d_rp;
     TRY(dalloc(e, &d_tb, nt + 1));
     TRY(dalloc(e, &d_ts, nt));
-    TRY(dalloc(e, &d_tpo, nt + 1));
-    TRY(dalloc(e, &d_ps, pair_src.size()));
-    TRY(dalloc(e, &d_pb, pair_base.size()));
-    TRY(dalloc(e, &d_pd, pair_doff.size()));
-    TRY(dalloc(e, &d_et, ent_tgt.size()));
-    TRY(dalloc(e, &d_ew, ent_w.size()));
-    CK(cudaMemcpy(d_tb, tile_beg.data(), 4 * (nt + 1), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d_ts, tile_scale.data(), 4 * nt, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d_tpo, tile_pair_off.data(), 8 * (nt + 1), cudaMemcpyHostToDevice));
-    if (!pair_src.empty()) {
-        CK(cudaMemcpy(d_ps, pair_src.data(), 4 * pair_src.size(), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(d_pb, pair_base.data(), 8 * pair_base.size(), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(d_pd, pair_doff.data(), 2 * pair_doff.size(), cudaMemcpyHostToDevice));
-    }
-    if (!ent_tgt.empty()) {
-        CK(cudaMemcpy(d_et, ent_tgt.data(), 2 * ent_tgt.size(), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(d_ew, ent_w.data(), 4 * ent_w.size(), cudaMemcpyHostToDevice));
+    TRY(dalloc(e, &d_tro, nt + 1));
+    TRY(dalloc(e, &d_tu, nt));
+    TRY(dalloc(e, &d_rs, nr));
+    TRY(dalloc(e, &d_rn, nr));
+    TRY(dalloc(e, &d_rp, nr));
+    TRY(dalloc(e, &d_ru, nr));
+    CK(cudaMemcpy(d_tb, th.tile_beg.data(), 4 * (nt + 1), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_ts, th.tile_scale.data(), 4 * nt, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_tro, th.tile_run_off.data(), 4 * (nt + 1), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_tu, th.tile_units.data(), 4 * nt, cudaMemcpyHostToDevice));
+    if (nr) {
+        CK(cudaMemcpy(d_rs, th.run_src0.data(), 4 * nr, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d_rn, th.run_n.data(), 4 * nr, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d_rp, th.run_pair0.data(), 8 * nr, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d_ru, th.run_unit0.data(), 4 * nr, cudaMemcpyHostToDevice));
     }
     a.n_tiles = nt;
-    a.tile_max = tile_max;
+    a.tile_max = th.tile_max;
     a.tile_beg = d_tb;
     a.tile_scale = d_ts;
-    a.tile_pair_off = d_tpo;
-    a.pair_src = d_ps;
-    a.pair_base = d_pb;
-    a.pair_doff = d_pd;
-    a.ent_tgt = d_et;
-    a.ent_w = d_ew;
+    a.tile_run_off = d_tro;
+    a.tile_units = d_tu;
+    a.run_src0 = d_rs;
+    a.run_n = d_rn;
+    a.run_pair0 = d_rp;
+    a.run_unit0 = d_ru;
     return BSIM_OK;
 }
 
 // Host construction of the tiled copy: synapses sorted by (tile of target,
-// source, delay); one pair per distinct (tile, source).
+// source, delay); one pair per distinct (tile, source), runs of consecutive
+// sources.
 static int build_tiles_host(Engine &e, const int32_t *inst, const int32_t *src, const int32_t *dst,
                             const float *weight, const int32_t *delay, int64_t s)
 {
     const int64_t n = e.N;
     const int32_t D = e.D;
+    std::vector<int64_t> indeg(n, 0);
+    for (int64_t k = 0; k < s; k++)
+        if (++indeg[dst[k]] > 65535) return fail(BSIM_ERR_LIMIT, "tiled delivery: a neuron has more than 65535 synapses in");
     std::vector<int64_t> runs = {0};
     for (int64_t i = 1; i < n; i++)
         if (inst && inst[i] != inst[i - 1]) runs.push_back(i);
     runs.push_back(n);
-    std::vector<int32_t> tile_beg;
-    int32_t tile_max = 0;
-    plan_tiles(runs, auto_tile_size(e.opt, n, e.sm_count), tile_beg, tile_max);
-    const int32_t nt = (int32_t)tile_beg.size() - 1;
+    TileHost th;
+    plan_tiles(runs, auto_tile_size(e.opt, n, e.sm_count), th.tile_beg, th.tile_max);
+    const int32_t nt = (int32_t)th.tile_beg.size() - 1;
     std::vector<int32_t> tile_of(n);
     for (int32_t q = 0; q < nt; q++)
-        for (int64_t i = tile_beg[q]; i < tile_beg[q + 1]; i++) tile_of[i] = q;
+        for (int64_t i = th.tile_beg[q]; i < th.tile_beg[q + 1]; i++) tile_of[i] = q;
     std::vector<std::pair<uint64_t, int64_t>> key(s);
     for (int64_t k = 0; k < s; k++)
         key[k] = {((uint64_t)tile_of[dst[k]] << 37) | ((uint64_t)src[k] << 6) | (uint64_t)(delay[k] - 1), k};
     std::sort(key.begin(), key.end());
-    std::vector<float> tile_scale(nt);
-    for (int32_t q = 0; q < nt; q++) tile_scale[q] = ldexpf(1.0f, e.qexp[inst ? inst[tile_beg[q]] : 0]);
-    std::vector<int64_t> tile_pair_off(nt + 1, 0);
-    std::vector<uint32_t> pair_src;
+    th.tile_scale.resize(nt);
+    for (int32_t q = 0; q < nt; q++) th.tile_scale[q] = ldexpf(1.0f, e.qexp[inst ? inst[th.tile_beg[q]] : 0]);
+    th.tile_run_off.assign(nt + 1, 0);
+    th.tile_units.assign(0, 0);
     std::vector<int64_t> pair_base;
     std::vector<uint16_t> pair_doff;
     std::vector<uint16_t> ent_tgt(s);
     std::vector<float> ent_w(s);
-    int64_t cur_pair_key = -1;
-    std::vector<int64_t> cnt(D + 1);
-    auto close_pair = [&]() -> bool {
-        if (cur_pair_key < 0) return true;
+    std::vector<int64_t> cnt(D);
+    int32_t cur_tile = -1;
+    int64_t cur_src = -1, run_start_src = -1, run_pair0 = 0;
+    auto close_pair = [&]() {
         int64_t c = 0;
         for (int d = 0; d <= D; d++) {
-            if (d > 0) c += cnt[d - 1];
-            if (c > 65535) return false;
             pair_doff.push_back((uint16_t)c);
+            if (d < D) c += cnt[d];
         }
-        return true;
+        std::fill(cnt.begin(), cnt.end(), 0);
+    };
+    auto close_run = [&]() {
+        if (run_start_src >= 0) add_run(th, (uint32_t)run_start_src, (int32_t)(cur_src - run_start_src + 1), run_pair0, D);
+    };
+    auto open_tiles_until = [&](int32_t q) {
+        while ((int32_t)th.tile_units.size() <= q) {
+            th.tile_units.push_back(0);
+            const int32_t qq = (int32_t)th.tile_units.size() - 1;
+            th.tile_run_off[qq + 1] = th.tile_run_off[qq];
+        }
     };
     for (int64_t pos = 0; pos < s; pos++) {
         const int64_t k = key[pos].second;
-        const int64_t pk = (int64_t)(key[pos].first >> 6);
         const int32_t q = tile_of[dst[k]];
-        if (pk != cur_pair_key) {
-            if (!close_pair()) return fail(BSIM_ERR_LIMIT, "tiled delivery: more than 65535 synapses of one source into one tile");
-            std::fill(cnt.begin(), cnt.end(), 0);
-            cur_pair_key = pk;
-            pair_src.push_back((uint32_t)src[k]);
+        if (q != cur_tile || src[k] != cur_src) {
+            if (cur_src >= 0) close_pair();
+            const bool extends = q == cur_tile && src[k] == cur_src + 1;
+            if (!extends) {
+                if (cur_tile >= 0) close_run();
+                open_tiles_until(q);
+                run_start_src = src[k];
+                run_pair0 = (int64_t)pair_base.size();
+            }
+            cur_tile = q;
+            cur_src = src[k];
             pair_base.push_back(pos);
-            tile_pair_off[q + 1] = (int64_t)pair_src.size();
         }
         cnt[delay[k] - 1]++;
-        ent_tgt[pos] = (uint16_t)(dst[k] - tile_beg[q]);
+        ent_tgt[pos] = (uint16_t)(dst[k] - th.tile_beg[q]);
         ent_w[pos] = weight[k];
     }
-    if (!close_pair()) return fail(BSIM_ERR_LIMIT, "tiled delivery: more than 65535 synapses of one source into one tile");
-    for (int32_t q = 0; q < nt; q++) tile_pair_off[q + 1] = std::max(tile_pair_off[q + 1], tile_pair_off[q]);
-    return upload_tiles(e, tile_beg, tile_max, tile_scale, tile_pair_off, pair_src, pair_base, pair_doff, ent_tgt,
-                        ent_w);
+    if (cur_src >= 0) {
+        close_pair();
+        close_run();
+    }
+    open_tiles_until(nt - 1);
+    int64_t *d_pb;
+    uint16_t *d_pd, *d_et;
+    float *d_ew;
+    TRY(dalloc(e, &d_pb, pair_base.size()));
+    TRY(dalloc(e, &d_pd, pair_doff.size()));
+    TRY(dalloc(e, &d_et, s));
+    TRY(dalloc(e, &d_ew, s));
+    if (!pair_base.empty()) {
+        CK(cudaMemcpy(d_pb, pair_base.data(), 8 * pair_base.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d_pd, pair_doff.data(), 2 * pair_doff.size(), cudaMemcpyHostToDevice));
+    }
+    if (s) {
+        CK(cudaMemcpy(d_et, ent_tgt.data(), 2 * s, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d_ew, ent_w.data(), 4 * s, cudaMemcpyHostToDevice));
+    }
+    e.a.pair_base = d_pb;
+    e.a.pair_doff = d_pd;
+    e.a.ent_tgt = d_et;
+    e.a.ent_w = d_ew;
+    return upload_tiles(e, th);
 }
 
 // ---------------------------------------------------------------------------
@@ -760,7 +808,7 @@ static __device__ __forceinline__ int find_seg(const TileSeg *segs, int n_segs, 
 // One warp per (tile, source) pair. Pass 0: per-delay counts -> cumulative
 // pair_doff and pair_cnt. Pass 1: entries in delay order, targets ascending.
 template <int PASS>
-__global__ void gen_tile_kernel(const TileSeg *segs, int n_segs, int64_t n_pairs, int D, uint32_t *pair_src,
+__global__ void gen_tile_kernel(const TileSeg *segs, int n_segs, int64_t n_pairs, int D,
                                 int64_t *pair_cnt, uint16_t *pair_doff, const int64_t *pair_base,
                                 uint16_t *ent_tgt, float *ent_w)
 {
@@ -801,7 +849,6 @@ __global__ void gen_tile_kernel(const TileSeg *segs, int n_segs, int64_t n_pairs
                 if (d < D) c += cur[d];
             }
             pair_cnt[k] = c;
-            pair_src[k] = (uint32_t)(sg.src_base + i);
         }
         __syncwarp();
     }
@@ -1008,7 +1055,9 @@ static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, co
         E.a.csc_d = d_cd;
     }
     // target-tiled copy
-    const bool tiles = wants_tiles(E.opt, D);
+    // four 16-bit limbs per sum cannot overflow while every in-degree is < 65,536
+    const bool tiles = wants_tiles(E.opt, D) &&
+                       *std::max_element(maxdeg.begin(), maxdeg.end()) <= 65535ull;
     if (tiles) {
         std::vector<int64_t> runs;
         for (int k = 0; k < ns; k++) runs.push_back(gi[k].nbase);
@@ -1018,16 +1067,20 @@ static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, co
         plan_tiles(runs, auto_tile_size(E.opt, N, E.sm_count), tile_beg, tile_max);
         const int32_t nt = (int32_t)tile_beg.size() - 1;
         std::vector<TileSeg> segs;
-        std::vector<int64_t> tile_pair_off(nt + 1);
-        std::vector<float> tile_scale(nt);
+        TileHost th;
+        th.tile_beg = tile_beg;
+        th.tile_max = tile_max;
+        th.tile_scale.resize(nt);
+        th.tile_run_off.assign(nt + 1, 0);
         int64_t pairs = 0;
         int k = 0;
         for (int32_t q = 0; q < nt; q++) {
             while (k + 1 < ns && gi[k + 1].nbase <= tile_beg[q]) k++;
             const GenInst &x = gi[k];
             const GenPlan &pl = plans[k];
-            tile_pair_off[q] = pairs;
-            tile_scale[q] = ldexpf(1.0f, E.qexp[k]);
+            th.tile_units.push_back(0);
+            th.tile_run_off[q + 1] = th.tile_run_off[q];
+            th.tile_scale[q] = ldexpf(1.0f, E.qexp[k]);
             const int64_t lb = tile_beg[q] - x.nbase, le = tile_beg[q + 1] - x.nbase;
             for (int64_t pp = lb / x.n; pp <= (le - 1) / x.n; pp++) {
                 const int64_t pop_beg = pp * x.n;
@@ -1049,31 +1102,27 @@ static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, co
                     sg.d_inst = x.D;
                     sg.pad = 0;
                     segs.push_back(sg);
+                    add_run(th, (uint32_t)sg.src_base, x.n, pairs, D);
                     pairs += x.n;
                 }
             }
         }
-        tile_pair_off[nt] = pairs;
         TileSeg *d_segs;
         int64_t *d_pcnt;
         if ((rc = talloc((void **)&d_segs, sizeof(TileSeg) * std::max<size_t>(1, segs.size()))) ||
             (rc = talloc((void **)&d_pcnt, sizeof(int64_t) * (pairs + 1)))) { free_tmp(); return bail(rc); }
         if (!segs.empty()) cudaMemcpy(d_segs, segs.data(), sizeof(TileSeg) * segs.size(), cudaMemcpyHostToDevice);
-        int32_t *d_tb; float *d_ts, *d_ew; int64_t *d_tpo, *d_pb; uint32_t *d_ps; uint16_t *d_pd, *d_et;
-        if ((rc = dalloc(E, &d_tb, nt + 1)) || (rc = dalloc(E, &d_ts, nt)) || (rc = dalloc(E, &d_tpo, nt + 1)) ||
-            (rc = dalloc(E, &d_ps, pairs)) || (rc = dalloc(E, &d_pb, pairs + 1)) ||
-            (rc = dalloc(E, &d_pd, (size_t)pairs * (D + 1))) || (rc = dalloc(E, &d_et, S)) || (rc = dalloc(E, &d_ew, S))) {
+        int64_t *d_pb; uint16_t *d_pd, *d_et; float *d_ew;
+        if ((rc = dalloc(E, &d_pb, pairs + 1)) || (rc = dalloc(E, &d_pd, (size_t)pairs * (D + 1))) ||
+            (rc = dalloc(E, &d_et, S)) || (rc = dalloc(E, &d_ew, S))) {
             free_tmp();
             return bail(rc);
         }
-        cudaMemcpy(d_tb, tile_beg.data(), 4 * (nt + 1), cudaMemcpyHostToDevice);
-        cudaMemcpy(d_ts, tile_scale.data(), 4 * nt, cudaMemcpyHostToDevice);
-        cudaMemcpy(d_tpo, tile_pair_off.data(), 8 * (nt + 1), cudaMemcpyHostToDevice);
-        gen_tile_kernel<0><<<gb, 256, 0, E.stream>>>(d_segs, (int)segs.size(), pairs, D, d_ps, d_pcnt, d_pd, nullptr,
+        gen_tile_kernel<0><<<gb, 256, 0, E.stream>>>(d_segs, (int)segs.size(), pairs, D, d_pcnt, d_pd, nullptr,
                                                     nullptr, nullptr);
         cudaMemcpyAsync(d_pb, d_pcnt, sizeof(int64_t) * pairs, cudaMemcpyDeviceToDevice, E.stream);
         if ((rc = scan(d_pb, pairs))) { free_tmp(); return bail(rc); }
-        gen_tile_kernel<1><<<gb, 256, 0, E.stream>>>(d_segs, (int)segs.size(), pairs, D, d_ps, d_pcnt, d_pd, d_pb,
+        gen_tile_kernel<1><<<gb, 256, 0, E.stream>>>(d_segs, (int)segs.size(), pairs, D, d_pcnt, d_pd, d_pb,
                                                     d_et, d_ew);
         int64_t tot = -1;
         cudaMemcpyAsync(&tot, d_pb + pairs, 8, cudaMemcpyDeviceToHost, E.stream);
@@ -1081,17 +1130,11 @@ static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, co
             free_tmp();
             return bail(fail(BSIM_ERR_CUDA, "generator: tiled copy does not match the synapse count"));
         }
-        StepArgs &a = E.a;
-        a.n_tiles = nt;
-        a.tile_max = tile_max;
-        a.tile_beg = d_tb;
-        a.tile_scale = d_ts;
-        a.tile_pair_off = d_tpo;
-        a.pair_src = d_ps;
-        a.pair_base = d_pb;
-        a.pair_doff = d_pd;
-        a.ent_tgt = d_et;
-        a.ent_w = d_ew;
+        E.a.pair_base = d_pb;
+        E.a.pair_doff = d_pd;
+        E.a.ent_tgt = d_et;
+        E.a.ent_w = d_ew;
+        if ((rc = upload_tiles(E, th))) { free_tmp(); return bail(rc); }
     }
     // push rows (not needed when every step uses the tiled copy)
     if (!(tiles && E.opt.delivery == BSIM_DELIVERY_TILE)) {

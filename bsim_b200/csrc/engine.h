@@ -65,18 +65,22 @@ struct StepArgs {
     // per-population spike counts of the last hist_len steps (predictor input)
     int32_t *pop_hist;          // [hist_len][n_pops]
     int32_t n_pops, hist_len;
-    // target-tiled delivery (BSIM_DELIVERY_TILE)
+    // target-tiled delivery (BSIM_DELIVERY_TILE). A tile's sources form runs of
+    // consecutive neuron ids; every source of a run owns one (tile, source) pair.
     int32_t n_tiles;
     int32_t tile_max;                // largest tile (neurons): shared-memory accumulator size
     const int32_t *tile_beg;         // [n_tiles + 1] first target of each tile
     const float *tile_scale;         // [n_tiles] 2^qexp of the tile's network
-    const int64_t *tile_pair_off;    // [n_tiles + 1] range of (tile, source) pairs
-    const uint32_t *pair_src;        // [P] source neuron of each pair
+    const int32_t *tile_run_off;     // [n_tiles + 1] range of runs
+    const int32_t *tile_units;       // [n_tiles] work units: sum over runs of ceil(n/32) * D
+    const uint32_t *run_src0;        // [runs] first source
+    const int32_t *run_n;            // [runs] sources in the run
+    const int64_t *run_pair0;        // [runs] pair of the first source
+    const int32_t *run_unit0;        // [runs] first work unit, counted within the tile
     const int64_t *pair_base;        // [P] first entry of each pair
     const uint16_t *pair_doff;       // [P][D + 1] cumulative entry counts by delay
     const uint16_t *ent_tgt;         // [S] target, relative to the tile's first neuron
     const float *ent_w;              // [S] weight
-    unsigned long long *fire_hist;   // [2][N] bit d-1 = fired d cycles ago (parity double-buffered)
 };
 
 struct Engine {

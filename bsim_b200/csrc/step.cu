@@ -101,11 +101,6 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
             st.w = __int_as_float(refrac);
             a.state[j] = st;
             if (hist) pop = __ldg(&c->pop);
-            if (a.fire_hist) {
-                // per-neuron shift register of the last 64 cycles (tiled delivery's source filter)
-                const unsigned long long old = a.fire_hist[(int64_t)(p ^ 1) * a.N + j];
-                a.fire_hist[(int64_t)p * a.N + j] = (old << 1) | (fired ? 1ull : 0ull);
-            }
         }
         const unsigned mask = __ballot_sync(0xffffffffu, fired);
         if (lane == 0 && base < a.N) bm[base >> 5] = mask;
@@ -351,47 +346,85 @@ static __device__ __forceinline__ unsigned long long pull_phase(const StepArgs &
 
 // ---------------------------------------------------------------------------
 // Phase B, tiled: each block owns a contiguous tile of target neurons and sums
-// their input exactly in shared memory (int64 fixed point), so no global atomic
-// is issued; the tile is written out once at the end. The tile's synapses are
-// grouped by (source, delay): a warp takes 32 (tile, source) pairs, filters them
-// with each source's fire history (bit d-1: fired d cycles ago), gathers the
-// active (pair, delay) segments into a per-warp list and streams their entries
-// ({u16 target offset, f32 weight}) as one flat range.
+// their input exactly in shared memory, so no global atomic is issued; the
+// tile is written out once at the end.
+//
+// The tile's synapses are grouped by (source, delay) and its sources form runs
+// of consecutive ids. A work unit is (run, delay d, 32-source chunk): one lane
+// reads the chunk's word of the fired bitmap of cycle t-d. Each fired
+// (source, delay) names one segment of entries ({u16 target offset, f32
+// weight}); a warp gathers up to TILE_SEGS segments and streams their entries
+// as one flat range, each lane advancing its own segment cursor.
+//
+// Exact sums with 32-bit shared atomics: the int64 fixed-point value of each
+// weight is split into four 16-bit limbs added into four u32 counters. A
+// target gets at most its in-degree (< 65,536, checked at build) inputs per
+// cycle, so no counter can overflow, and sum_k (counter_k << 16k) mod 2^64 is
+// the exact two's-complement sum.
 // ---------------------------------------------------------------------------
 #define TILE_SEGS 64
 
-static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &a, int p, int pw,
-                                                                unsigned long long *s_acc, long long *s_start,
-                                                                int *s_cum)
+// Counters are limb-major ([4][2 * tile]: limb k of sum i at k * stride + i) so
+// that lanes adding into scattered targets spread over all shared-memory banks.
+static __device__ __forceinline__ void limb_add(unsigned *c, int stride, long long v)
+{
+    const unsigned long long u = (unsigned long long)v;
+    atomicAdd(c, (unsigned)(u & 0xFFFFull));
+    atomicAdd(c + stride, (unsigned)((u >> 16) & 0xFFFFull));
+    atomicAdd(c + 2 * stride, (unsigned)((u >> 32) & 0xFFFFull));
+    atomicAdd(c + 3 * stride, (unsigned)(u >> 48));
+}
+
+static __device__ __forceinline__ long long limb_sum(const unsigned *c, int stride)
+{
+    const unsigned long long u = (unsigned long long)c[0] + ((unsigned long long)c[stride] << 16) +
+                                 ((unsigned long long)c[2 * stride] << 32) +
+                                 ((unsigned long long)c[3 * stride] << 48);
+    return (long long)u;
+}
+
+static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &a, unsigned long long t, int pw,
+                                                                unsigned *s_acc, long long *s_start, int *s_cum)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int D = a.D;
-    const unsigned long long dmask = D >= 64 ? ~0ull : ((1ull << D) - 1ull);
     long long *seg_start = s_start + warp * TILE_SEGS;
     int *seg_cum = s_cum + warp * TILE_SEGS;
-    const unsigned long long *hist = a.fire_hist + (int64_t)(p ^ 1) * a.N;  // state after cycle t-1
     unsigned long long ev = 0;
     for (int q = blockIdx.x; q < a.n_tiles; q += gridDim.x) {
         const int tb = a.tile_beg[q], T = a.tile_beg[q + 1] - tb;
-        for (int i = threadIdx.x; i < 2 * T; i += blockDim.x) s_acc[i] = 0ull;
+        for (int i = threadIdx.x; i < 8 * T; i += blockDim.x) s_acc[i] = 0u;
         __syncthreads();
         const float sc = a.tile_scale[q];
-        const int64_t k0 = a.tile_pair_off[q], k1 = a.tile_pair_off[q + 1];
-        for (int64_t kb = k0 + (int64_t)warp * 32; kb < k1; kb += (int64_t)nwarps * 32) {
-            const int64_t k = kb + lane;
-            unsigned long long m = 0;
-            int64_t pbase = 0;
-            const uint16_t *doff = nullptr;
-            if (k < k1) {
-                m = hist[a.pair_src[k]] & dmask;
-                if (m) {
-                    pbase = a.pair_base[k];
-                    doff = a.pair_doff + k * (D + 1);
+        const int r0 = a.tile_run_off[q], r1 = a.tile_run_off[q + 1];
+        const int n_units = a.tile_units[q];
+        for (int ub = warp * 32; ub < n_units; ub += nwarps * 32) {
+            const int u = ub + lane;
+            unsigned m = 0;
+            int64_t kbase = 0;
+            int d = 1;
+            if (u < n_units) {
+                int r = r0;
+                while (r + 1 < r1 && a.run_unit0[r + 1] <= u) r++;
+                const int n_r = a.run_n[r], chunks = (n_r + 31) >> 5;
+                const int v = u - a.run_unit0[r];
+                d = v / chunks + 1;
+                const int c = v - (d - 1) * chunks;
+                if ((long long)t - d >= 0) {
+                    const int64_t s_first = (int64_t)a.run_src0[r] + 32 * c;
+                    const int len = min(32, n_r - 32 * c);
+                    const uint32_t *bm = a.bitmap + (int64_t)((t - d) % (unsigned long long)a.R) * a.W;
+                    const int64_t wi = s_first >> 5;
+                    const int sh = (int)(s_first & 31);
+                    unsigned bits = bm[wi];
+                    if (sh) bits = (bits >> sh) | ((wi + 1 < a.W ? bm[wi + 1] : 0u) << (32 - sh));
+                    m = len == 32 ? bits : (bits & ((1u << len) - 1u));
+                    kbase = a.run_pair0[r] + 32 * c;
                 }
             }
             while (__any_sync(0xffffffffu, m != 0)) {
-                // this round: up to TILE_SEGS (pair, delay) segments of the warp
-                const int cnt = __popcll(m);
+                // this round: up to TILE_SEGS fired (source, delay) segments of the warp
+                const int cnt = __popc(m);
                 int incl = cnt;
 #pragma unroll
                 for (int o = 1; o < 32; o <<= 1) {
@@ -402,18 +435,19 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
                 const int total = __shfl_sync(0xffffffffu, incl, 31);
                 const int take = max(0, min(cnt, TILE_SEGS - excl));
                 for (int i = 0; i < take; i++) {
-                    const int b = __ffsll((long long)m) - 1;
+                    const int b = __ffs(m) - 1;
                     m &= m - 1;
-                    const int e0 = doff[b], e1 = doff[b + 1];
-                    seg_start[excl + i] = pbase + e0;
+                    const int64_t k = kbase + b;
+                    const uint16_t *doff = a.pair_doff + k * (D + 1);
+                    const int e0 = doff[d - 1], e1 = doff[d];
+                    seg_start[excl + i] = a.pair_base[k] + e0;
                     seg_cum[excl + i] = e1 - e0;  // length for now
                 }
                 __syncwarp();
                 const int nseg = min(total, TILE_SEGS);
                 // inclusive prefix of the segment lengths (two per lane)
-                int l0 = lane < nseg ? seg_cum[lane] : 0;
-                int l1 = lane + 32 < nseg ? seg_cum[lane + 32] : 0;
-                int c0 = l0, c1 = l1;
+                int c0 = lane < nseg ? seg_cum[lane] : 0;
+                int c1 = lane + 32 < nseg ? seg_cum[lane + 32] : 0;
 #pragma unroll
                 for (int o = 1; o < 32; o <<= 1) {
                     const int n0 = __shfl_up_sync(0xffffffffu, c0, o);
@@ -430,31 +464,25 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
                 __syncwarp();
                 const int n_ent = seg_cum[nseg - 1];
                 if (lane == 0) ev += (unsigned long long)n_ent;
+                int j = 0;  // this lane's segment cursor (its flat positions only grow)
                 for (int f0 = 0; f0 < n_ent; f0 += 4 * 32) {
                     uint16_t tg[4];
                     float wv[4];
-                    bool ok[4];
 #pragma unroll
-                    for (int u = 0; u < 4; u++) {
-                        const int f = f0 + u * 32 + lane;
-                        ok[u] = f < n_ent;
-                        if (ok[u]) {
-                            int lo = 0, hi = nseg - 1;
-                            while (lo < hi) {
-                                const int mid = (lo + hi) >> 1;
-                                if (seg_cum[mid] > f) hi = mid;
-                                else lo = mid + 1;
-                            }
-                            const int64_t e = seg_start[lo] + (f - (lo ? seg_cum[lo - 1] : 0));
-                            tg[u] = __ldcs(a.ent_tgt + e);
-                            wv[u] = __ldcs(a.ent_w + e);
+                    for (int uu = 0; uu < 4; uu++) {
+                        const int f = f0 + uu * 32 + lane;
+                        if (f < n_ent) {
+                            while (seg_cum[j] <= f) j++;
+                            const int64_t e = seg_start[j] + (f - (j ? seg_cum[j - 1] : 0));
+                            tg[uu] = __ldcs(a.ent_tgt + e);
+                            wv[uu] = __ldcs(a.ent_w + e);
                         }
                     }
 #pragma unroll
-                    for (int u = 0; u < 4; u++) {
-                        if (ok[u]) {
-                            const long long qv = __float2ll_rn(__fmul_rn(wv[u], sc));
-                            atomicAdd(s_acc + 2 * (int)tg[u] + (wv[u] >= 0.0f ? 0 : 1), (unsigned long long)qv);
+                    for (int uu = 0; uu < 4; uu++) {
+                        if (f0 + uu * 32 + lane < n_ent) {
+                            const long long qv = __float2ll_rn(__fmul_rn(wv[uu], sc));
+                            limb_add(s_acc + 2 * (int)tg[uu] + (wv[uu] >= 0.0f ? 0 : 1), 2 * T, qv);
                         }
                     }
                 }
@@ -464,7 +492,7 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
         __syncthreads();
         longlong2 *g = reinterpret_cast<longlong2 *>(a.acc) + (int64_t)pw * a.N + tb;
         for (int i = threadIdx.x; i < T; i += blockDim.x)
-            g[i] = make_longlong2((long long)s_acc[2 * i], (long long)s_acc[2 * i + 1]);
+            g[i] = make_longlong2(limb_sum(s_acc + 2 * i, 2 * T), limb_sum(s_acc + 2 * i + 1, 2 * T));
         __syncthreads();
     }
     return ev;
@@ -503,7 +531,7 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const StepAr
     __shared__ PushSeg s_seg[MAX_WARPS * PUSH_CHUNK];
     __shared__ int s_wcnt[64];
     __shared__ unsigned long long s_ev;
-    // tiled delivery: [2 * tile_max] u64 accumulators, then per-warp segment lists
+    // tiled delivery: [4][2 * tile] u32 limb counters, then per-warp segment lists
     extern __shared__ __align__(16) unsigned long long s_dyn[];
     const unsigned long long t = *reinterpret_cast<volatile unsigned long long *>(a.step_ctr);
     const int p = (int)(t & 1ull);
@@ -529,9 +557,9 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const StepAr
     if (push) {
         ev = push_phase(a, t, p ^ 1, s_cum, s_seg);
     } else if (tiled) {
-        long long *starts = reinterpret_cast<long long *>(s_dyn + 2 * a.tile_max);
+        long long *starts = reinterpret_cast<long long *>(s_dyn + 4 * a.tile_max);
         int *cums = reinterpret_cast<int *>(starts + MAX_WARPS * TILE_SEGS);
-        ev = tile_phase(a, p, p ^ 1, s_dyn, starts, cums);
+        ev = tile_phase(a, t, p ^ 1, reinterpret_cast<unsigned *>(s_dyn), starts, cums);
     } else {
         ev = pull_phase<ACC>(a, t, p ^ 1);
     }
@@ -588,8 +616,7 @@ __global__ void record_flush_kernel(const StepArgs a)
 size_t step_dynamic_smem(const StepArgs &a)
 {
     if (a.n_tiles == 0) return 0;
-    return (size_t)2 * a.tile_max * sizeof(unsigned long long) +
-           (size_t)MAX_WARPS * TILE_SEGS * (sizeof(long long) + sizeof(int));
+    return (size_t)8 * a.tile_max * sizeof(unsigned) + (size_t)MAX_WARPS * TILE_SEGS * (sizeof(long long) + sizeof(int));
 }
 
 // The attribute belongs to the kernel, not to an engine: it only ever grows,
