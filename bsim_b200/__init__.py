@@ -48,7 +48,8 @@ class GenSpec(ctypes.Structure):
                 ("v_init_lo", ctypes.c_float), ("v_init_hi", ctypes.c_float),
                 ("v_rest", ctypes.c_float), ("v_reset", ctypes.c_float), ("cm", ctypes.c_float),
                 ("tau_m", ctypes.c_float), ("tau_refrac", ctypes.c_float), ("tau_syn_E", ctypes.c_float),
-                ("tau_syn_I", ctypes.c_float), ("v_thresh", ctypes.c_float)]
+                ("tau_syn_I", ctypes.c_float), ("v_thresh", ctypes.c_float),
+                ("drive_scale", ctypes.c_float), ("drive_half_period", ctypes.c_int32)]
 
 
 class Info(ctypes.Structure):
@@ -64,8 +65,25 @@ EXPORTS = [
     "bsim_options_default", "bsim_create", "bsim_create_generated", "bsim_gen_count", "bsim_gen_host",
     "bsim_synapse_reset", "bsim_run", "bsim_run_async", "bsim_sync", "bsim_record", "bsim_read_raster",
     "bsim_read_state", "bsim_read_fire_count", "bsim_read_pop_counts", "bsim_get_info", "bsim_get_qexp",
-    "bsim_destroy", "bsim_last_error", "bsim_write_state", "bsim_get_stream",
+    "bsim_destroy", "bsim_last_error", "bsim_write_state", "bsim_get_stream", "bsim_set_drive",
+    "bsim_enable_pop_stats", "bsim_read_pop_info", "bsim_mlp_init", "bsim_mlp_forward", "bsim_mlp_grad",
+    "bsim_mlp_train", "bsim_set_predictor", "bsim_predictor_stats", "bsim_autotune",
 ]
+
+MLP_IN = 9
+MLP_HIDDEN = 64
+MLP_PARAMS = MLP_HIDDEN * MLP_IN + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN + MLP_HIDDEN + 1
+
+
+class PredStats(ctypes.Structure):
+    _fields_ = [("cycles", ctypes.c_int64), ("fallbacks", ctypes.c_int64), ("tile_cycles", ctypes.c_int64),
+                ("abs_err_sum", ctypes.c_double), ("actual_sum", ctypes.c_double)]
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("block_threads", ctypes.c_int32), ("grid_blocks", ctypes.c_int32), ("delivery", ctypes.c_int32),
+                ("best_us_per_step", ctypes.c_float), ("cost_push", ctypes.c_float * 2),
+                ("cost_tile", ctypes.c_float * 2), ("candidates", ctypes.c_int32)]
 
 _lib = None
 
@@ -99,6 +117,16 @@ def lib():
             "bsim_destroy": [P],
             "bsim_write_state": [P, P, P, P, P],
             "bsim_get_stream": [P, P],
+            "bsim_set_drive": [P, P, i32],
+            "bsim_enable_pop_stats": [P, i32],
+            "bsim_read_pop_info": [P, P, P, P],
+            "bsim_mlp_init": [P, ctypes.c_uint64],
+            "bsim_mlp_forward": [P, P, i64, P],
+            "bsim_mlp_grad": [P, P, P, i64, P, P],
+            "bsim_mlp_train": [P, P, P, i64, i32, i32, f32, ctypes.c_uint64, P],
+            "bsim_set_predictor": [P, P, f32, P, P],
+            "bsim_predictor_stats": [P, P],
+            "bsim_autotune": [P, i32, P],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -135,7 +163,7 @@ def gen_spec(**kw):
     d = dict(seed=1, n_pop=10, pop_size=1000, p_conn=0.1, remote_frac=0.2, max_delay=6, exc_frac=0.8,
              w_max=1e-10, inh_scale=4.0, i_min=0.0, i_max=1.1e-9, v_init_lo=-65e-3, v_init_hi=-50e-3,
              v_rest=-65e-3, v_reset=-65e-3, cm=0.25e-9, tau_m=20e-3, tau_refrac=2e-3, tau_syn_E=5e-3,
-             tau_syn_I=10e-3, v_thresh=-50e-3)
+             tau_syn_I=10e-3, v_thresh=-50e-3, drive_scale=1.0, drive_half_period=0)
     d.update(kw)
     s = GenSpec()
     for k, v in d.items():
@@ -157,6 +185,39 @@ def gen_host(spec):
     d = np.zeros(s, np.int32)
     _check(lib().bsim_gen_host(ctypes.byref(spec), _p(params), _p(pop), _p(src), _p(dst), _p(w), _p(d)))
     return dict(params=params, pop=pop, src=src, dst=dst, weight=w, delay_steps=d)
+
+
+def mlp_init(seed=1):
+    p = np.zeros(MLP_PARAMS, np.float32)
+    _check(lib().bsim_mlp_init(_p(p), seed))
+    return p
+
+
+def mlp_forward(params, x):
+    params = np.ascontiguousarray(params, np.float32)
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.zeros(x.shape[0], np.float32)
+    _check(lib().bsim_mlp_forward(_p(params), _p(x), x.shape[0], _p(y)))
+    return y
+
+
+def mlp_grad(params, x, y):
+    params = np.ascontiguousarray(params, np.float32)
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    g = np.zeros(MLP_PARAMS, np.float32)
+    loss = ctypes.c_float()
+    _check(lib().bsim_mlp_grad(_p(params), _p(x), _p(y), x.shape[0], _p(g), ctypes.byref(loss)))
+    return g, loss.value
+
+
+def mlp_train(params, x, y, epochs=20, batch=256, lr=1e-3, seed=1):
+    params = np.array(params, np.float32)
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    loss = ctypes.c_float()
+    _check(lib().bsim_mlp_train(_p(params), _p(x), _p(y), x.shape[0], epochs, batch, lr, seed, ctypes.byref(loss)))
+    return params, loss.value
 
 
 def synapse_reset(delay_s, weight, tau_syn, dt):
@@ -236,6 +297,43 @@ class Engine:
         c = lambda a, t: None if a is None else np.ascontiguousarray(a, t)
         v, i_E, i_I, refrac = c(v, np.float32), c(i_E, np.float32), c(i_I, np.float32), c(refrac, np.int32)
         _check(lib().bsim_write_state(self._h, _p(v), _p(i_E), _p(i_I), _p(refrac)))
+
+    def set_drive(self, params_hi, half_period):
+        p = np.ascontiguousarray(params_hi, np.float32)
+        _check(lib().bsim_set_drive(self._h, _p(p), half_period))
+
+    def enable_pop_stats(self, hist_len=64):
+        _check(lib().bsim_enable_pop_stats(self._h, hist_len))
+
+    def pop_counts(self, steps):
+        P = self.info().n_pops
+        c = np.zeros((steps, P), np.int32)
+        _check(lib().bsim_read_pop_counts(self._h, _p(c), steps))
+        return c
+
+    def pop_info(self):
+        P = self.info().n_pops
+        size = np.zeros(P, np.int32)
+        ind = np.zeros(P, np.float32)
+        outd = np.zeros(P, np.float32)
+        _check(lib().bsim_read_pop_info(self._h, _p(size), _p(ind), _p(outd)))
+        return size, ind, outd
+
+    def set_predictor(self, params, tolerance=0.25, cost_push=None, cost_tile=None):
+        cp = None if cost_push is None else np.ascontiguousarray(cost_push, np.float32)
+        ct = None if cost_tile is None else np.ascontiguousarray(cost_tile, np.float32)
+        pp = None if params is None else np.ascontiguousarray(params, np.float32)
+        _check(lib().bsim_set_predictor(self._h, _p(pp), tolerance, _p(cp), _p(ct)))
+
+    def predictor_stats(self):
+        st = PredStats()
+        _check(lib().bsim_predictor_stats(self._h, ctypes.byref(st)))
+        return st
+
+    def autotune(self, trial_steps=50):
+        r = TuneResult()
+        _check(lib().bsim_autotune(self._h, trial_steps, ctypes.byref(r)))
+        return r
 
     def stream(self):
         """The engine's cudaStream_t as an integer handle (for torch.cuda.ExternalStream)."""

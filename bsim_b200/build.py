@@ -12,7 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libbsim_b200.so")
-SOURCES = ["csrc/step.cu", "csrc/build.cu", "csrc/noalloc.cu"]
+SOURCES = ["csrc/step.cu", "csrc/build.cu", "csrc/noalloc.cu", "csrc/predictor.cu"]
 HEADERS = ["csrc/engine.h", "csrc/netgen.h", "../include/bsim_b200.h"]
 
 

@@ -209,6 +209,7 @@ static int create_from_arrays(const float *params, int64_t n, const int32_t *pop
     e->N = n;
     e->S = s;
     e->D = D;
+    e->dt = dt;
     e->n_inst = n_inst;
     e->n_pops = n_pops;
     e->qexp = qexp;
@@ -390,7 +391,8 @@ static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
     a.step_ctr = d_ctr;
     a.events = d_ctr + 1;
     a.ticket = reinterpret_cast<unsigned int *>(d_ctr + 2);
-    a.delivery = e.opt.delivery == BSIM_DELIVERY_PULL ? BSIM_DELIVERY_PULL : BSIM_DELIVERY_PUSH;
+    a.delivery = (e.opt.delivery == BSIM_DELIVERY_PULL || e.opt.delivery == BSIM_DELIVERY_AUTO) ? e.opt.delivery
+                                                                                                 : BSIM_DELIVERY_PUSH;
     a.deliv_sel = nullptr;
     a.rec_ids = nullptr;
     a.rec_off = nullptr;
@@ -659,7 +661,7 @@ static __device__ __forceinline__ int find_inst(const GenDev &g, int64_t gid)
 // Per-neuron state, v_tmp and class id. rm and Cm come from the host fold of
 // each class so v_tmp = (i_offset*rm + v_rest) * (1 - Cm) rounds as on the host.
 __global__ void gen_neurons_kernel(GenDev g, const bsim_gen_spec *specs, const float *cls_rm, const float *cls_Cm,
-                                   float4 *state, float *vtmp, uint16_t *cls, int64_t N)
+                                   float4 *state, float *vtmp, float *vtmp_alt, uint16_t *cls, int64_t N)
 {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
         const int k = find_inst(g, i);
@@ -674,6 +676,12 @@ __global__ void gen_neurons_kernel(GenDev g, const bsim_gen_spec *specs, const f
         float vt = __fadd_rn(__fmul_rn(ioff, rm), sp.v_rest);
         vt = __fmul_rn(vt, __fsub_rn(1.0f, Cm));
         vtmp[i] = vt;
+        if (vtmp_alt) {
+            // square-wave drive: the odd half periods' i_offset is i_offset * drive_scale
+            const float ioff_hi = sp.drive_half_period > 0 ? __fmul_rn(ioff, sp.drive_scale) : ioff;
+            float va = __fadd_rn(__fmul_rn(ioff_hi, rm), sp.v_rest);
+            vtmp_alt[i] = __fmul_rn(va, __fsub_rn(1.0f, Cm));
+        }
         cls[i] = (uint16_t)c;
         state[i] = make_float4(vinit, 0.0f, 0.0f, 0.0f);
     }
@@ -971,6 +979,7 @@ static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, co
     if (rc != BSIM_OK) { free_engine(e); return rc; }
     e->N = N;
     e->D = D;
+    e->dt = dt;
     e->n_inst = ns;
     e->n_cls = n_cls;
     e->n_pops = n_cls;
@@ -1000,10 +1009,22 @@ static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, co
     cudaMemcpy(d_Cm, cls_Cm.data(), sizeof(float) * n_cls, cudaMemcpyHostToDevice);
     GenDev gd{d_gi, ns, d_proj, d_in, d_out, D};
 
-    float4 *d_state; float *d_vtmp; uint16_t *d_cls;
-    if ((rc = dalloc(E, &d_state, N)) || (rc = dalloc(E, &d_vtmp, N)) || (rc = dalloc(E, &d_cls, N))) { free_tmp(); return bail(rc); }
+    int32_t drive_half = 0;
+    for (int k = 0; k < ns; k++) {
+        const int32_t h = specs[k].drive_half_period;
+        if (h < 0 || (h > 0 && drive_half > 0 && h != drive_half)) {
+            free_tmp();
+            return bail(fail(BSIM_ERR_ARG, "generator: networks of one engine must share the drive half period"));
+        }
+        if (h > 0) drive_half = h;
+    }
+    float4 *d_state; float *d_vtmp, *d_vtmp_alt = nullptr; uint16_t *d_cls;
+    if ((rc = dalloc(E, &d_state, N)) || (rc = dalloc(E, &d_vtmp, N)) || (rc = dalloc(E, &d_cls, N)) ||
+        (drive_half > 0 && (rc = dalloc(E, &d_vtmp_alt, N)))) { free_tmp(); return bail(rc); }
     const int gb = E.sm_count * 8;
-    gen_neurons_kernel<<<gb, 256, 0, E.stream>>>(gd, d_specs, d_rm, d_Cm, d_state, d_vtmp, d_cls, N);
+    gen_neurons_kernel<<<gb, 256, 0, E.stream>>>(gd, d_specs, d_rm, d_Cm, d_state, d_vtmp, d_vtmp_alt, d_cls, N);
+    E.a.vtmp_alt = d_vtmp_alt;
+    E.a.drive_half = drive_half;
 
     // in-degree and max |w| per instance -> fixed-point exponents
     int64_t *d_col;
@@ -1428,6 +1449,30 @@ int bsim_write_state(bsim_engine *eh, const float *v, const float *iE, const flo
     return BSIM_OK;
 }
 
+int bsim_set_drive(bsim_engine *eh, const float *params_hi, int32_t half_period)
+{
+    if (!eh || half_period < 0 || (half_period > 0 && !params_hi)) return fail(BSIM_ERR_ARG, "bsim_set_drive: invalid arguments");
+    Engine &e = *H(eh);
+    CK(cudaSetDevice(e.device));
+    CK(cudaStreamSynchronize(e.stream));
+    if (half_period > 0) {
+        std::vector<float> vt(e.N);
+        const float dt = e.dt;
+        for (int64_t i = 0; i < e.N; i++) vt[i] = fold_lif(params_hi + 10 * i, dt).v_tmp;
+        if (!e.a.vtmp_alt) {
+            float *d;
+            TRY(dalloc(e, &d, e.N));
+            e.a.vtmp_alt = d;
+        }
+        CK(cudaMemcpy(const_cast<float *>(e.a.vtmp_alt), vt.data(), sizeof(float) * e.N, cudaMemcpyHostToDevice));
+    }
+    e.a.drive_half = half_period;
+    // the captured graph holds the old arguments
+    if (e.graph_exec) { cudaGraphExecDestroy(e.graph_exec); e.graph_exec = nullptr; }
+    if (e.graph) { cudaGraphDestroy(e.graph); e.graph = nullptr; }
+    return BSIM_OK;
+}
+
 int bsim_get_stream(bsim_engine *eh, void **stream)
 {
     if (!eh || !stream) return fail(BSIM_ERR_ARG, "invalid arguments");
@@ -1445,12 +1490,264 @@ int bsim_read_fire_count(bsim_engine *eh, int32_t *count)
     return BSIM_OK;
 }
 
+static void drop_graph(Engine &e)
+{
+    if (e.graph_exec) { cudaGraphExecDestroy(e.graph_exec); e.graph_exec = nullptr; }
+    if (e.graph) { cudaGraphDestroy(e.graph); e.graph = nullptr; }
+}
+
+// Per-population size and summed in/out degree, from whichever copies of the
+// synapses the engine holds (push rows, pull rows or the tiled copy).
+__global__ void pop_degree_kernel(StepArgs a, int32_t *size, double *in_sum, double *out_sum)
+{
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < a.N; j += (int64_t)gridDim.x * blockDim.x) {
+        const int pop = a.ctab[a.cls[j]].pop;
+        atomicAdd(&size[pop], 1);
+        if (a.col_off) atomicAdd(&in_sum[pop], (double)(a.col_off[j + 1] - a.col_off[j]));
+        if (a.row_off) atomicAdd(&out_sum[pop], (double)(a.row_off[(j + 1) * a.D] - a.row_off[j * a.D]));
+    }
+}
+
+__global__ void pop_degree_tiles_kernel(StepArgs a, double *in_sum, double *out_sum, int want_in, int want_out)
+{
+    // one block per tile: entries per pair give out-degree of the source and in-degree of the tile
+    for (int q = blockIdx.x; q < a.n_tiles; q += gridDim.x) {
+        for (int r = a.tile_run_off[q]; r < a.tile_run_off[q + 1]; r++) {
+            for (int i = threadIdx.x; i < a.run_n[r]; i += blockDim.x) {
+                const int64_t k = a.run_pair0[r] + i;
+                const double c = (double)a.pair_doff[k * (a.D + 1) + a.D];
+                const uint32_t src = a.run_src0[r] + i;
+                if (want_out) atomicAdd(&out_sum[a.ctab[a.cls[src]].pop], c);
+                if (want_in) atomicAdd(&in_sum[a.ctab[a.cls[a.tile_beg[q]]].pop], c);
+            }
+        }
+    }
+}
+
+static int ensure_pop_info(Engine &e)
+{
+    if (e.pop_info_ready) return BSIM_OK;
+    const int P = e.n_pops;
+    int32_t *d_size;
+    double *d_in, *d_out;
+    float *d_ind, *d_outd;
+    TRY(dalloc(e, &d_size, P));
+    TRY(dalloc(e, &d_in, P));
+    TRY(dalloc(e, &d_out, P));
+    TRY(dalloc(e, &d_ind, P));
+    TRY(dalloc(e, &d_outd, P));
+    CK(cudaMemset(d_size, 0, 4 * P));
+    CK(cudaMemset(d_in, 0, 8 * P));
+    CK(cudaMemset(d_out, 0, 8 * P));
+    pop_degree_kernel<<<e.sm_count * 4, 256, 0, e.stream>>>(e.a, d_size, d_in, d_out);
+    if (e.a.n_tiles > 0 && (!e.a.col_off || !e.a.row_off))
+        pop_degree_tiles_kernel<<<e.sm_count * 4, 256, 0, e.stream>>>(e.a, d_in, d_out, e.a.col_off ? 0 : 1,
+                                                                      e.a.row_off ? 0 : 1);
+    CK(cudaStreamSynchronize(e.stream));
+    std::vector<int32_t> sz(P);
+    std::vector<double> in(P), out(P);
+    std::vector<float> ind(P), outd(P);
+    CK(cudaMemcpy(sz.data(), d_size, 4 * P, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(in.data(), d_in, 8 * P, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(out.data(), d_out, 8 * P, cudaMemcpyDeviceToHost));
+    for (int p = 0; p < P; p++) {
+        ind[p] = sz[p] ? (float)(in[p] / sz[p]) : 0.0f;
+        outd[p] = sz[p] ? (float)(out[p] / sz[p]) : 0.0f;
+    }
+    CK(cudaMemcpy(d_ind, ind.data(), 4 * P, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_outd, outd.data(), 4 * P, cudaMemcpyHostToDevice));
+    e.a.pop_size = d_size;
+    e.a.pop_indeg = d_ind;
+    e.a.pop_outdeg = d_outd;
+    e.pop_info_ready = true;
+    return BSIM_OK;
+}
+
+int bsim_enable_pop_stats(bsim_engine *eh, int32_t hist_len)
+{
+    if (!eh || hist_len < 16) return fail(BSIM_ERR_ARG, "bsim_enable_pop_stats: hist_len must be >= 16");
+    Engine &e = *H(eh);
+    CK(cudaSetDevice(e.device));
+    CK(cudaStreamSynchronize(e.stream));
+    TRY(ensure_pop_info(e));
+    if (e.a.pop_hist && e.a.hist_len == hist_len) return BSIM_OK;
+    int32_t *h;
+    TRY(dalloc(e, &h, (size_t)hist_len * e.n_pops));
+    CK(cudaMemset(h, 0, sizeof(int32_t) * hist_len * e.n_pops));
+    e.a.pop_hist = h;
+    e.a.hist_len = hist_len;
+    drop_graph(e);
+    return BSIM_OK;
+}
+
 int bsim_read_pop_counts(bsim_engine *eh, int32_t *counts, int32_t steps)
 {
-    (void)counts;
-    (void)steps;
+    if (!eh || !counts || steps < 0) return fail(BSIM_ERR_ARG, "bsim_read_pop_counts: invalid arguments");
+    Engine &e = *H(eh);
+    if (!e.a.pop_hist) return fail(BSIM_ERR_STATE, "population statistics are not enabled on this engine");
+    if (steps > e.a.hist_len - 2) return fail(BSIM_ERR_ARG, "bsim_read_pop_counts: steps > hist_len - 2");
+    CK(cudaSetDevice(e.device));
+    CK(cudaStreamSynchronize(e.stream));
+    const int H = e.a.hist_len, P = e.n_pops;
+    std::vector<int32_t> ring((size_t)H * P);
+    CK(cudaMemcpy(ring.data(), e.a.pop_hist, sizeof(int32_t) * H * P, cudaMemcpyDeviceToHost));
+    const int64_t T = e.steps_done;
+    for (int32_t k = 0; k < steps; k++) {
+        const int64_t s = T - steps + k;
+        for (int p = 0; p < P; p++) counts[(int64_t)k * P + p] = s >= 0 ? ring[(size_t)(s % H) * P + p] : 0;
+    }
+    return BSIM_OK;
+}
+
+int bsim_read_pop_info(bsim_engine *eh, int32_t *size, float *mean_indeg, float *mean_outdeg)
+{
     if (!eh) return fail(BSIM_ERR_ARG, "null engine");
-    return fail(BSIM_ERR_STATE, "population statistics are not enabled on this engine");
+    Engine &e = *H(eh);
+    CK(cudaSetDevice(e.device));
+    CK(cudaStreamSynchronize(e.stream));
+    TRY(ensure_pop_info(e));
+    const int P = e.n_pops;
+    if (size) CK(cudaMemcpy(size, e.a.pop_size, 4 * P, cudaMemcpyDeviceToHost));
+    if (mean_indeg) CK(cudaMemcpy(mean_indeg, e.a.pop_indeg, 4 * P, cudaMemcpyDeviceToHost));
+    if (mean_outdeg) CK(cudaMemcpy(mean_outdeg, e.a.pop_outdeg, 4 * P, cudaMemcpyDeviceToHost));
+    return BSIM_OK;
+}
+
+int bsim_set_predictor(bsim_engine *eh, const float *params, float tolerance, const float *cost_push,
+                       const float *cost_tile)
+{
+    if (!eh || (params && !(tolerance >= 0))) return fail(BSIM_ERR_ARG, "bsim_set_predictor: invalid arguments");
+    Engine &e = *H(eh);
+    CK(cudaSetDevice(e.device));
+    CK(cudaStreamSynchronize(e.stream));
+    if (!params) {
+        e.a.mlp = nullptr;
+        drop_graph(e);
+        return BSIM_OK;
+    }
+    if (!e.a.pop_hist) return fail(BSIM_ERR_STATE, "bsim_set_predictor: enable population statistics first");
+    if (!e.a.pred_ring) {
+        float *w, *ring, *sum;
+        PredStats *ps;
+        TRY(dalloc(e, &w, BSIM_MLP_PARAMS));
+        TRY(dalloc(e, &ring, 4 * (size_t)e.n_pops));
+        TRY(dalloc(e, &sum, 8));
+        TRY(dalloc(e, &ps, 1));
+        e.a.mlp = w;
+        e.a.pred_ring = ring;
+        e.a.pred_sum = sum;
+        e.a.pstats = ps;
+    }
+    CK(cudaMemcpy(const_cast<float *>(e.a.mlp), params, sizeof(float) * BSIM_MLP_PARAMS, cudaMemcpyHostToDevice));
+    CK(cudaMemset(e.a.pred_ring, 0, sizeof(float) * 4 * e.n_pops));
+    CK(cudaMemset(e.a.pred_sum, 0, sizeof(float) * 8));
+    CK(cudaMemset(e.a.pstats, 0, sizeof(PredStats)));
+    e.a.pred_tol = tolerance;
+    e.a.mean_outdeg = e.N ? (float)((double)e.S / (double)e.N) : 0.0f;
+    e.a.cost_push_a = cost_push ? cost_push[0] : 0.0f;
+    e.a.cost_push_b = cost_push ? cost_push[1] : 1.0f;
+    e.a.cost_tile_a = cost_tile ? cost_tile[0] : 0.0f;
+    e.a.cost_tile_b = cost_tile ? cost_tile[1] : 2.0f;
+    drop_graph(e);
+    return BSIM_OK;
+}
+
+int bsim_predictor_stats(bsim_engine *eh, bsim_pred_stats *st)
+{
+    if (!eh || !st) return fail(BSIM_ERR_ARG, "invalid arguments");
+    Engine &e = *H(eh);
+    memset(st, 0, sizeof(*st));
+    if (!e.a.pstats) return BSIM_OK;
+    CK(cudaSetDevice(e.device));
+    CK(cudaStreamSynchronize(e.stream));
+    PredStats ps;
+    CK(cudaMemcpy(&ps, e.a.pstats, sizeof(ps), cudaMemcpyDeviceToHost));
+    st->cycles = (int64_t)ps.cycles;
+    st->fallbacks = (int64_t)ps.fallbacks;
+    st->tile_cycles = (int64_t)ps.tile_cycles;
+    st->abs_err_sum = ps.abs_err;
+    st->actual_sum = ps.actual;
+    return BSIM_OK;
+}
+
+int bsim_autotune(bsim_engine *eh, int32_t trial_steps, bsim_tune_result *out)
+{
+    if (!eh || trial_steps < 1 || !out) return fail(BSIM_ERR_ARG, "bsim_autotune: invalid arguments");
+    Engine &e = *H(eh);
+    CK(cudaSetDevice(e.device));
+    CK(cudaStreamSynchronize(e.stream));
+    memset(out, 0, sizeof(*out));
+    if (e.opt.accumulate == BSIM_ACC_ORDERED) {  // one schedule only
+        out->block_threads = e.block;
+        out->grid_blocks = e.grid;
+        out->delivery = BSIM_DELIVERY_PULL;
+        return BSIM_OK;
+    }
+    std::vector<int> modes;
+    if (e.a.row_off) modes.push_back(BSIM_DELIVERY_PUSH);
+    if (e.a.n_tiles > 0) modes.push_back(BSIM_DELIVERY_TILE);
+    const int saved_block = e.block, saved_grid = e.grid, saved_del = e.a.delivery;
+    const size_t smem = step_dynamic_smem(e.a);
+    cudaEvent_t ev0, ev1;
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+    float best = 1e30f;
+    int best_b = saved_block, best_g = saved_grid, best_m = saved_del;
+    float mode_best[4] = {1e30f, 1e30f, 1e30f, 1e30f};
+    unsigned long long mode_ev[4] = {0, 0, 0, 0};
+    const int blocks[2] = {256, 512};
+    for (int m : modes) {
+        for (int b : blocks) {
+            int bps = 0;
+            if (step_occupancy(b, e.opt.accumulate, &bps, smem) != cudaSuccess || bps < 1) continue;
+            const int grids[2] = {e.sm_count * bps, e.sm_count};
+            for (int g : grids) {
+                e.block = b;
+                e.grid = g;
+                e.a.delivery = m;
+                unsigned long long c0[2], c1[2];
+                CK(cudaMemcpy(c0, e.a.step_ctr, sizeof(c0), cudaMemcpyDeviceToHost));
+                CK(cudaEventRecord(ev0, e.stream));
+                for (int k = 0; k < trial_steps; k++) CK(launch_step(e));
+                CK(cudaEventRecord(ev1, e.stream));
+                CK(cudaEventSynchronize(ev1));
+                float ms = 0.0f;
+                CK(cudaEventElapsedTime(&ms, ev0, ev1));
+                CK(cudaMemcpy(c1, e.a.step_ctr, sizeof(c1), cudaMemcpyDeviceToHost));
+                e.steps_done += trial_steps;
+                out->candidates++;
+                const float us = 1e3f * ms / trial_steps;
+                if (us < best) {
+                    best = us;
+                    best_b = b;
+                    best_g = g;
+                    best_m = m;
+                }
+                if (us < mode_best[m]) {
+                    mode_best[m] = us;
+                    mode_ev[m] = (c1[1] - c0[1]) / (unsigned long long)trial_steps;
+                }
+            }
+        }
+    }
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    e.block = best_b;
+    e.grid = best_g;
+    e.a.delivery = best_m;
+    e.opt.delivery = best_m;
+    drop_graph(e);
+    out->block_threads = best_b;
+    out->grid_blocks = best_g;
+    out->delivery = best_m;
+    out->best_us_per_step = best;
+    // cost model of each mode: ns per event at the trial's activity (fixed part not separated)
+    if (mode_best[BSIM_DELIVERY_PUSH] < 1e29f && mode_ev[BSIM_DELIVERY_PUSH] > 0)
+        out->cost_push[1] = 1e3f * mode_best[BSIM_DELIVERY_PUSH] / (float)mode_ev[BSIM_DELIVERY_PUSH];
+    if (mode_best[BSIM_DELIVERY_TILE] < 1e29f && mode_ev[BSIM_DELIVERY_TILE] > 0)
+        out->cost_tile[1] = 1e3f * mode_best[BSIM_DELIVERY_TILE] / (float)mode_ev[BSIM_DELIVERY_TILE];
+    (void)saved_del;
+    return BSIM_OK;
 }
 
 int bsim_get_info(bsim_engine *eh, bsim_info *info)

@@ -30,6 +30,12 @@ struct RecCtl {
     long long cap;
 };
 
+// Firing-predictor statistics, accumulated on the device.
+struct PredStats {
+    unsigned long long cycles, fallbacks, tile_cycles;
+    double abs_err, actual;
+};
+
 // Everything one fused step launch needs. Passed by value (kernel parameter space).
 struct StepArgs {
     int64_t N;         // neurons
@@ -39,6 +45,8 @@ struct StepArgs {
     int64_t W;         // bitmap words per ring slot = ceil(N / 32)
     float4 *state;     // [N] {v, i_E, i_I, refrac_step as int bits}
     const float *vtmp; // [N]
+    const float *vtmp_alt;  // [N] v_tmp of the odd half periods of a square-wave drive (may be NULL)
+    int32_t drive_half;     // cycles per half period (0: constant drive)
     const uint16_t *cls;       // [N] class of each neuron
     const ClassParams *ctab;   // [n_cls]
     void *acc;                 // [2][N] longlong2 (EXACT) or float2 (ORDERED): input for the next step
@@ -81,6 +89,16 @@ struct StepArgs {
     const uint16_t *pair_doff;       // [P][D + 1] cumulative entry counts by delay
     const uint16_t *ent_tgt;         // [S] target, relative to the tile's first neuron
     const float *ent_w;              // [S] weight
+    // firing predictor (needs pop_hist)
+    const float *mlp;                // [BSIM_MLP_PARAMS] (NULL: off)
+    const int32_t *pop_size;         // [n_pops]
+    const float *pop_indeg;          // [n_pops] mean in-degree
+    const float *pop_outdeg;         // [n_pops] mean out-degree
+    float *pred_ring;                // [4][n_pops] predicted spikes of cycle s at slot s % 4
+    float *pred_sum;                 // [4][2] predicted spikes and events of cycle s at slot s % 4
+    PredStats *pstats;
+    float pred_tol, mean_outdeg;
+    float cost_push_a, cost_push_b, cost_tile_a, cost_tile_b;  // ns per cycle, ns per event
 };
 
 struct Engine {
@@ -90,6 +108,7 @@ struct Engine {
     int sm_count = 0;
     int64_t N = 0, S = 0;
     int32_t D = 1;
+    float dt = 0.0f;
     int32_t n_inst = 1, n_cls = 0, n_pops = 1;
     std::vector<int32_t> qexp;  // per instance
     int64_t steps_done = 0;
@@ -104,6 +123,8 @@ struct Engine {
     // recording
     int64_t rec_cap_alloc = 0, rec_steps_alloc = 0;
     bool rec_dirty = false;
+    // population statistics (device arrays in a: pop_size, pop_indeg, pop_outdeg)
+    bool pop_info_ready = false;
 };
 
 }  // namespace bsim

@@ -56,6 +56,7 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
     int32_t *slot_ids = a.ring + (int64_t)cur * a.cap;
     uint32_t *bm = a.bitmap + (int64_t)cur * a.W;
     int32_t *hist = a.pop_hist ? a.pop_hist + (int64_t)(t % (unsigned long long)a.hist_len) * a.n_pops : nullptr;
+    const float *vtmp = (a.drive_half > 0 && ((t / (unsigned long long)a.drive_half) & 1ull)) ? a.vtmp_alt : a.vtmp;
     for (int64_t bbase = (int64_t)blockIdx.x * blockDim.x; bbase < a.N; bbase += stride) {
         const int64_t base = bbase + (threadIdx.x & ~31);
         const int64_t j = base + lane;
@@ -82,7 +83,7 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
                 refrac -= 1;  // input of this cycle is dropped
             } else {
                 const float Cm = __ldg(&c->Cm), C_E = __ldg(&c->C_E), C_I = __ldg(&c->C_I);
-                float v = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(Cm, st.x), a.vtmp[j]), __fmul_rn(st.y, C_E)),
+                float v = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(Cm, st.x), vtmp[j]), __fmul_rn(st.y, C_E)),
                                     __fmul_rn(st.z, C_I));
                 float iE = __fmul_rn(__ldg(&c->CE), st.y);
                 float iI = __fmul_rn(__ldg(&c->CI), st.z);
@@ -498,6 +499,91 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
     return ev;
 }
 
+// ---------------------------------------------------------------------------
+// Firing predictor, inside the step: one warp per population evaluates the MLP
+// on the population's rates of cycles t-1..t-8 (complete when cycle t runs) and
+// its mean in-degree, predicting cycle t+1. Lane u holds hidden units u and
+// u+32; the second layer reads the first layer's units through shuffles. The
+// prediction only feeds scheduling (the delivery choice of later cycles).
+// ---------------------------------------------------------------------------
+static __device__ __forceinline__ void predict_phase(const StepArgs &a, unsigned long long t)
+{
+    const int lane = threadIdx.x & 31;
+    const float *P = a.mlp;
+    const float *W1 = P, *b1 = P + BSIM_MLP_HIDDEN * BSIM_MLP_IN, *W2 = b1 + BSIM_MLP_HIDDEN;
+    const float *b2 = W2 + BSIM_MLP_HIDDEN * BSIM_MLP_HIDDEN, *W3 = b2 + BSIM_MLP_HIDDEN, *b3 = W3 + BSIM_MLP_HIDDEN;
+    const int H = a.hist_len;
+    for (int p = ((int)(blockIdx.x * blockDim.x + threadIdx.x)) >> 5; p < a.n_pops;
+         p += (int)((gridDim.x * blockDim.x) >> 5)) {
+        const float size = (float)a.pop_size[p];
+        float x[BSIM_MLP_IN];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const long long s = (long long)t - 1 - k;
+            x[k] = s >= 0 ? (float)a.pop_hist[(int64_t)(s % H) * a.n_pops + p] / size * 10.0f : 0.0f;
+        }
+        x[8] = a.pop_indeg[p] * 1e-3f;
+        float h1a = b1[lane], h1b = b1[lane + 32];
+#pragma unroll
+        for (int k = 0; k < BSIM_MLP_IN; k++) {
+            h1a = fmaf(W1[lane * BSIM_MLP_IN + k], x[k], h1a);
+            h1b = fmaf(W1[(lane + 32) * BSIM_MLP_IN + k], x[k], h1b);
+        }
+        h1a = fmaxf(h1a, 0.0f);
+        h1b = fmaxf(h1b, 0.0f);
+        float s_a = b2[lane], s_b = b2[lane + 32];
+        for (int k = 0; k < 32; k++) {
+            const float ha = __shfl_sync(0xffffffffu, h1a, k), hb = __shfl_sync(0xffffffffu, h1b, k);
+            s_a = fmaf(W2[lane * BSIM_MLP_HIDDEN + k], ha, s_a);
+            s_a = fmaf(W2[lane * BSIM_MLP_HIDDEN + 32 + k], hb, s_a);
+            s_b = fmaf(W2[(lane + 32) * BSIM_MLP_HIDDEN + k], ha, s_b);
+            s_b = fmaf(W2[(lane + 32) * BSIM_MLP_HIDDEN + 32 + k], hb, s_b);
+        }
+        float y = W3[lane] * fmaxf(s_a, 0.0f) + W3[lane + 32] * fmaxf(s_b, 0.0f);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+        if (lane == 0) {
+            const float pred = fmaxf(y + b3[0], 0.0f) * size * 0.1f;
+            a.pred_ring[(int64_t)((t + 1) & 3) * a.n_pops + p] = pred;
+            atomicAdd(&a.pred_sum[((t + 1) & 3) * 2 + 0], pred);
+            atomicAdd(&a.pred_sum[((t + 1) & 3) * 2 + 1], pred * a.pop_outdeg[p]);
+            if (t >= 3) {
+                // the prediction made two cycles ago for cycle t-1, now complete
+                const float actual = (float)a.pop_hist[(int64_t)((t - 1) % H) * a.n_pops + p];
+                const float predicted = a.pred_ring[(int64_t)((t - 1) & 3) * a.n_pops + p];
+                atomicAdd(&a.pstats->abs_err, (double)fabsf(predicted - actual));
+                atomicAdd(&a.pstats->actual, (double)actual);
+            }
+        }
+    }
+}
+
+// The delivery mode of cycle t under BSIM_DELIVERY_AUTO: the cost model on the
+// predicted work, or on the exact spike count of cycle t-1 when the prediction
+// for that cycle missed by more than the tolerance (the fallback). Every block
+// computes the same choice from the same device words.
+static __device__ __forceinline__ int auto_delivery(const StepArgs &a, unsigned long long t)
+{
+    float ps = 0.0f, pe = 0.0f, as = 0.0f;
+    if (t >= 1) {
+        const float *slot = a.pred_sum + ((t - 1) & 3) * 2;
+        ps = *reinterpret_cast<const volatile float *>(slot);
+        pe = *reinterpret_cast<const volatile float *>(slot + 1);
+        as = (float)a.ring_cnt[(t - 1) % (unsigned long long)a.R];
+    }
+    const bool fallback = t < 3 || fabsf(as - ps) > a.pred_tol * fmaxf(ps, 1.0f);
+    const float work = (float)a.D * (fallback ? as * a.mean_outdeg : pe);
+    const int dm = (a.n_tiles > 0 && a.cost_tile_a + a.cost_tile_b * work < a.cost_push_a + a.cost_push_b * work)
+                       ? BSIM_DELIVERY_TILE
+                       : BSIM_DELIVERY_PUSH;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.pstats->cycles += 1;
+        a.pstats->fallbacks += fallback ? 1 : 0;
+        a.pstats->tile_cycles += dm == BSIM_DELIVERY_TILE ? 1 : 0;
+    }
+    return dm;
+}
+
 // Copies the complete ring slot of cycle t-1 into the raster recording.
 static __device__ __forceinline__ void record_phase(const StepArgs &a, unsigned long long t)
 {
@@ -537,7 +623,13 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const StepAr
     const int p = (int)(t & 1ull);
     const int cur = (int)(t % (unsigned long long)a.R);
     int dm = a.deliv_sel ? *a.deliv_sel : a.delivery;
+    if (dm == BSIM_DELIVERY_AUTO) dm = a.mlp ? auto_delivery(a, t) : BSIM_DELIVERY_PUSH;
     if (dm == BSIM_DELIVERY_TILE && a.n_tiles == 0) dm = BSIM_DELIVERY_PUSH;
+    if (a.mlp && blockIdx.x == 0 && threadIdx.x == 32) {
+        // slot t+2 is next written by cycle t+1's prediction
+        a.pred_sum[((t + 2) & 3) * 2 + 0] = 0.0f;
+        a.pred_sum[((t + 2) & 3) * 2 + 1] = 0.0f;
+    }
     const bool push = ACC != BSIM_ACC_ORDERED && dm == BSIM_DELIVERY_PUSH;
     const bool tiled = ACC != BSIM_ACC_ORDERED && dm == BSIM_DELIVERY_TILE;
     if (threadIdx.x == 0) s_ev = 0;
@@ -564,6 +656,7 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const StepAr
         ev = pull_phase<ACC>(a, t, p ^ 1);
     }
     if (ev) atomicAdd(&s_ev, ev);
+    if (a.mlp && a.pop_hist) predict_phase(a, t);
     __syncthreads();
     if (threadIdx.x == 0) {
         if (s_ev) atomicAdd(a.events, s_ev);

@@ -80,6 +80,10 @@ typedef struct bsim_gen_spec {
     float v_init_lo, v_init_hi; /* v_init U[lo, hi) per neuron */
     /* LIFENeuron parameters shared by all neurons (constructor order minus v_init, i_offset) */
     float v_rest, v_reset, cm, tau_m, tau_refrac, tau_syn_E, tau_syn_I, v_thresh;
+    /* Square-wave drive: in odd half periods every i_offset is multiplied by drive_scale
+     * (drive_half_period cycles per half period; 0 = constant drive). */
+    float drive_scale;
+    int32_t drive_half_period;
 } bsim_gen_spec;
 
 typedef struct bsim_info {
@@ -168,12 +172,84 @@ int bsim_write_state(bsim_engine *e, const float *v, const float *i_E, const flo
 /* The CUDA stream (cudaStream_t) all of the engine's work is enqueued on. */
 int bsim_get_stream(bsim_engine *e, void **stream);
 
+/* Square-wave drive for an engine built from arrays: in odd half periods of
+ * half_period cycles, v_tmp is folded from params_hi ([n][10], normally differing
+ * from the creation parameters in i_offset only). half_period = 0 turns it off. */
+int bsim_set_drive(bsim_engine *e, const float *params_hi, int32_t half_period);
+
 /* Spikes per neuron since creation (FireInfo "count", src/sim/SingleGPUSimulator.cu:263-282). */
 int bsim_read_fire_count(bsim_engine *e, int32_t *count);
 
-/* Spike count of each population over the last `steps` recorded cycles
- * ([steps][n_pops], oldest first; at most the predictor history length). */
+/* Per-population spike statistics: keeps the spike count of every population for
+ * the last hist_len cycles (hist_len >= 16) in a device ring. */
+int bsim_enable_pop_stats(bsim_engine *e, int32_t hist_len);
+
+/* Spike count of each population over the last `steps` cycles ([steps][n_pops],
+ * oldest first; steps <= hist_len - 2). */
 int bsim_read_pop_counts(bsim_engine *e, int32_t *counts, int32_t steps);
+
+/* Size, mean in-degree and mean out-degree of each population ([n_pops] each; any may be NULL). */
+int bsim_read_pop_info(bsim_engine *e, int32_t *size, float *mean_indeg, float *mean_outdeg);
+
+/* ---- Firing predictor -------------------------------------------------------
+ * A small MLP predicts each population's rate two cycles ahead from its rates in
+ * the last 8 cycles and its mean in-degree. It only steers scheduling (delivery
+ * mode per cycle); it never touches the dynamics, so rasters are identical with
+ * and without it. Features and target (rates are spikes / size * 10, i.e. 1.0 per
+ * 1 kHz at dt = 0.1 ms): x = [r(t-1), ..., r(t-8), mean_indeg / 1000], y = r(t+1). */
+#define BSIM_MLP_IN 9
+#define BSIM_MLP_HIDDEN 64
+#define BSIM_MLP_PARAMS (BSIM_MLP_HIDDEN * BSIM_MLP_IN + BSIM_MLP_HIDDEN + BSIM_MLP_HIDDEN * BSIM_MLP_HIDDEN + \
+                         BSIM_MLP_HIDDEN + BSIM_MLP_HIDDEN + 1)
+/* Parameter layout: W1[64][9], b1[64], W2[64][64], b2[64], W3[64], b3. */
+
+/* Deterministic initialisation (uniform +-sqrt(6/(fan_in+fan_out)), zero biases). Host only. */
+int bsim_mlp_init(float *params, uint64_t seed);
+
+/* Forward pass on the GPU for n samples: x [n][9] -> y [n]. Host buffers. */
+int bsim_mlp_forward(const float *params, const float *x, int64_t n, float *y);
+
+/* Mean-squared-error loss and its gradient over n samples, on the GPU (the
+ * project's own backward kernel). grad [BSIM_MLP_PARAMS]. Host buffers. */
+int bsim_mlp_grad(const float *params, const float *x, const float *y_target, int64_t n, float *grad, float *loss);
+
+/* Adam training on the GPU (mini-batches of `batch`, learning rate lr) for
+ * `epochs` passes; params are read and updated in place. */
+int bsim_mlp_train(float *params, const float *x, const float *y_target, int64_t n, int32_t epochs, int32_t batch,
+                   float lr, uint64_t seed, float *final_loss);
+
+/* Attaches (params != NULL) or detaches (NULL) the predictor. Needs population
+ * statistics. With delivery BSIM_DELIVERY_AUTO the predicted events of the next
+ * cycle pick push or tiled delivery by the cost model (ns per event and fixed ns
+ * per cycle of each mode, e.g. from bsim_autotune); when the exact spike count of a
+ * cycle departs from its prediction by more than tolerance (relative), that
+ * cycle's choice is recomputed from the exact counts (a fallback). */
+int bsim_set_predictor(bsim_engine *e, const float *params, float tolerance, const float *cost_push,
+                       const float *cost_tile);
+
+typedef struct bsim_pred_stats {
+    int64_t cycles;          /* cycles scheduled by the predictor */
+    int64_t fallbacks;       /* cycles whose choice was recomputed from exact counts */
+    int64_t tile_cycles;     /* cycles delivered with the tiled mode */
+    double abs_err_sum;      /* sum over cycles and populations of |predicted - actual| spikes */
+    double actual_sum;       /* sum of actual spikes over the same cycles and populations */
+} bsim_pred_stats;
+
+int bsim_predictor_stats(bsim_engine *e, bsim_pred_stats *stats);
+
+/* Autotuner (replaces the occupancy rule of getBlockSize, src/gpu_utils/gpu_func.cu:90-127):
+ * runs trial_steps cycles for each candidate (block size, grid, delivery mode),
+ * keeps the fastest and reports each mode's measured cost. The simulation advances
+ * by the trial cycles (the dynamics are the same for every candidate). */
+typedef struct bsim_tune_result {
+    int32_t block_threads, grid_blocks, delivery;
+    float best_us_per_step;
+    float cost_push[2];      /* fixed ns per cycle, ns per event */
+    float cost_tile[2];
+    int32_t candidates;
+} bsim_tune_result;
+
+int bsim_autotune(bsim_engine *e, int32_t trial_steps, bsim_tune_result *out);
 
 int bsim_get_info(bsim_engine *e, bsim_info *info);
 

@@ -51,6 +51,11 @@ typedef struct oracle_out {
     void *final_state;      /* [n][4] REAL: v, i_E, i_I, refrac_step (as REAL) at the end */
     int64_t *spikes_per_step;  /* [steps] (may be NULL) */
     int64_t *events_per_step;  /* [steps] synaptic events delivered in each step (may be NULL) */
+    /* Optional square-wave drive (an input, kept here to leave the run signature
+     * stable): cycle t uses the v_tmp folded from params_alt ([n][10] REAL) when
+     * (t / half_period) is odd. params_alt may differ from params in i_offset only. */
+    const void *params_alt;
+    int64_t half_period;  /* 0: constant drive */
 } oracle_out;
 
 /* ---- float build (reference `real` = float) ---- */

@@ -112,12 +112,31 @@ int SFX(oracle_run)(const REAL *params, int64_t n,
     int64_t *ring_n = (int64_t *)calloc((size_t)R, sizeof(int64_t));
     int64_t ev_cap = 1024;
     int64_t *ev = (int64_t *)malloc(sizeof(int64_t) * (size_t)ev_cap);
+    REAL *vtmp_base = NULL, *vtmp_alt = NULL; /* square-wave drive: v_tmp of each phase */
     int rc = 0;
     if (!fold || !rtime || !rstep || !synE || !synI || !accE || !accI || !off || !ids || !ring || !ring_n || !ev) {
         rc = -4;
         goto done;
     }
     SFX(oracle_lif_reset)(params, n, dt, fold, rtime);
+    if (out->params_alt && out->half_period > 0) {
+        REAL *fa = (REAL *)malloc(sizeof(REAL) * ORACLE_NFOLD * (size_t)n);
+        int32_t *ra = (int32_t *)malloc(sizeof(int32_t) * (size_t)n);
+        vtmp_base = (REAL *)malloc(sizeof(REAL) * (size_t)n);
+        vtmp_alt = (REAL *)malloc(sizeof(REAL) * (size_t)n);
+        if (!fa || !ra || !vtmp_base || !vtmp_alt) {
+            free(fa); free(ra); free(vtmp_base); free(vtmp_alt);
+            rc = -4;
+            goto done;
+        }
+        SFX(oracle_lif_reset)((const REAL *)out->params_alt, n, dt, fa, ra);
+        for (int64_t j = 0; j < n; j++) {
+            vtmp_base[j] = fold[j * ORACLE_NFOLD + 5];
+            vtmp_alt[j] = fa[j * ORACLE_NFOLD + 5];
+        }
+        free(fa);
+        free(ra);
+    }
 
     /* Synapse ids grouped by (source, delay), creation order inside a group. */
     for (int64_t k = 0; k < s; k++) off[(int64_t)src[k] * D + (delay_steps[k] - 1) + 1]++;
@@ -138,6 +157,10 @@ int SFX(oracle_run)(const REAL *params, int64_t n,
         const int32_t slot = (int32_t)(t % R);
         int32_t *fired_list = ring + (int64_t)slot * n;
         int64_t nf = 0;
+        if (vtmp_alt && (t % out->half_period) == 0) {
+            const REAL *src_vt = ((t / out->half_period) & 1) ? vtmp_alt : vtmp_base;
+            for (int64_t j = 0; j < n; j++) fold[j * ORACLE_NFOLD + 5] = src_vt[j];
+        }
         for (int64_t j = 0; j < n; j++) {
             REAL *f = fold + j * ORACLE_NFOLD;
             REAL in_E, in_I;
@@ -239,6 +262,7 @@ int SFX(oracle_run)(const REAL *params, int64_t n,
         }
     }
 done:
+    free(vtmp_base); free(vtmp_alt);
     free(fold); free(rtime); free(rstep); free(synE); free(synI); free(accE); free(accI);
     free(off); free(ids); free(ring); free(ring_n); free(ev);
     return rc;

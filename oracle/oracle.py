@@ -70,6 +70,8 @@ class _Out(ctypes.Structure):
         ("final_state", ctypes.c_void_p),
         ("spikes_per_step", ctypes.c_void_p),
         ("events_per_step", ctypes.c_void_p),
+        ("params_alt", ctypes.c_void_p),
+        ("half_period", ctypes.c_int64),
     ]
 
 
@@ -104,9 +106,10 @@ def syn_reset(delay_s, weight, tau_syn, dt, dtype=np.float32):
 
 
 def run(params, src, dst, weight, delay_steps, dt, steps, record_steps=0, rec_ids=None,
-        acc_mode=ACC_SEQUENTIAL, qexp=None, dtype=np.float32, raster_cap=None):
+        acc_mode=ACC_SEQUENTIAL, qexp=None, dtype=np.float32, raster_cap=None, params_alt=None, half_period=0):
     """Run the oracle. Returns a dict with fire_count, raster (list of arrays),
-    v_trace [record_steps, n_rec], final_state [n, 4], spikes/events per step."""
+    v_trace [record_steps, n_rec], final_state [n, 4], spikes/events per step.
+    params_alt / half_period: square-wave drive (params_alt's v_tmp in odd half periods)."""
     params = np.ascontiguousarray(params, dtype=dtype)
     n = params.shape[0]
     src = np.ascontiguousarray(src, dtype=np.int32)
@@ -129,9 +132,11 @@ def run(params, src, dst, weight, delay_steps, dt, steps, record_steps=0, rec_id
     events = np.zeros(steps, dtype=np.int64)
     if qexp is not None:
         qexp = np.ascontiguousarray(np.broadcast_to(np.asarray(qexp, dtype=np.int32), (n,)))
+    if params_alt is not None:
+        params_alt = np.ascontiguousarray(params_alt, dtype=dtype)
     out = _Out(record_steps, _ptr(fire_count), _ptr(raster_off), _ptr(raster_ids), raster_cap,
                _ptr(rec_ids), rec_ids.shape[0], _ptr(v_trace), _ptr(final_state), _ptr(spikes),
-               _ptr(events))
+               _ptr(events), _ptr(params_alt), int(half_period))
     sfx = "f32" if dtype == np.float32 else "f64"
     rc = getattr(lib(), "oracle_run_" + sfx)(
         _ptr(params), n, _ptr(src), _ptr(dst), _ptr(weight), _ptr(delay_steps), s, dt, steps,

@@ -228,3 +228,28 @@ def test_tiled_batched_long_delays_equal_alone():
             mine = rb[t][(rb[t] >= base) & (rb[t] < base + n)] - base
             assert np.array_equal(mine, ra[t]), t
         base += n
+
+
+def test_square_wave_drive_vs_oracle():
+    """Square-wave drive (i_offset x drive_scale in odd half periods): device-built
+    and host-built (bsim_set_drive) engines both bit-exact against the oracle."""
+    spec = W.cuba(6, 500, 100, 6, seed=51)
+    spec.i_max = 1.0e-9
+    spec.drive_scale = 20.0
+    spec.drive_half_period = 60
+    g = B.gen_host(spec)
+    hi = g["params"].copy()
+    hi[:, 9] = (g["params"][:, 9] * np.float32(20.0)).astype(np.float32)
+    dev = B.Engine.generated(spec, DT)
+    host = engine_from(g)
+    host.set_drive(hi, 60)
+    rd, vd = run_checkpoints(dev, 300, 300)
+    rh, vh = run_checkpoints(host, 300, 300)
+    fx = oracle.run(g["params"], g["src"], g["dst"], g["weight"], g["delay_steps"], DT, 300, record_steps=300,
+                    rec_ids=np.arange(g["params"].shape[0]), acc_mode=oracle.ACC_FIXED,
+                    qexp=int(dev.qexp()[0]), params_alt=hi, half_period=60)
+    assert same_raster(rd, fx["raster"]) is None and same_raster(rh, fx["raster"]) is None
+    assert np.array_equal(vd[-1], fx["v_trace"][-1]) and np.array_equal(vh[-1], fx["v_trace"][-1])
+    lo_rate = sum(len(r) for r in fx["raster"][:60]) / 60
+    hi_rate = sum(len(r) for r in fx["raster"][60:120]) / 60
+    assert hi_rate > 3 * lo_rate
