@@ -206,6 +206,127 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+# Batched + predictor-scheduled vs plain
+# ---------------------------------------------------------------------------
+def batched_vs_plain(n_nets, steps, device):
+    """The networks of the batched generator (populations U{5..40} x neurons
+    U{500..8000}, 100/500/2000 Hz, delays U{1..6} or U{1..50}) run (a) one engine
+    per network with push delivery, one after the other (plain), and (b) all in
+    one engine with per-cycle delivery chosen by the trained firing predictor
+    (batched + predicted). Same cycles, same dynamics: every network's spike
+    counts are compared between (a) and (b)."""
+    import torch
+    import bsim_b200 as B
+    from bsim_b200 import predictor as PR
+    from bsim_b200 import workloads as W
+    specs, _ = W.batched(n_nets, seed=7)
+
+    def timed(eng, k):
+        st = torch.cuda.ExternalStream(eng.stream(), device=device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        i0 = eng.info().events_total
+        e0.record(st)
+        eng.run_async(k)
+        e1.record(st)
+        e1.synchronize()
+        eng.sync()
+        return e0.elapsed_time(e1), eng.info().events_total - i0
+
+    # predictor trained on a separate short trace (a different seed of a driven net)
+    t_train = time.perf_counter()
+    tr = W.cuba(10, 1000, 500, 6, seed=99, i_max=2e-9)
+    tr.drive_scale, tr.drive_half_period = 8.0, 500
+    counts, size, indeg = PR.collect([tr], 3000, DT, opts=B.options(device=device))
+    x, y = PR.features(counts, size, indeg)
+    params, loss = PR.train(x, y, epochs=10, batch=512, lr=2e-3)
+    t_train = time.perf_counter() - t_train
+
+    # Batched engines, one per delay range (an engine walks the delay slots of its
+    # longest delay for every spike), stepping concurrently on their own streams.
+    # Their autotuning trials advance them, and the plain runs are warmed up by the
+    # same number of cycles so that both end on the same cycle.
+    groups = {}
+    for i, sp in enumerate(specs):
+        groups.setdefault(sp.max_delay, []).append(i)
+    engines = []
+    for dmax, idx in sorted(groups.items()):
+        eb = B.Engine.generated([specs[i] for i in idx], DT,
+                                opts=B.options(device=device, graph_steps=100, delivery=B.DELIVERY_AUTO))
+        tune = eb.autotune(5)
+        eb.enable_pop_stats(64)
+        eb.set_predictor(params, tolerance=0.3, cost_push=list(tune.cost_push), cost_tile=list(tune.cost_tile))
+        engines.append((idx, eb, tune))
+    warm = max(int(eb.info().steps_done) for _, eb, _ in engines)
+    for _, eb, _ in engines:
+        eb.run(warm - int(eb.info().steps_done))
+    plain_ms, plain_ev, plain_counts = 0.0, 0, {}
+    for i, sp in enumerate(specs):
+        e = B.Engine.generated(sp, DT, opts=B.options(device=device, graph_steps=100))
+        e.run(warm)
+        ms, ev = timed(e, steps)
+        plain_ms += ms
+        plain_ev += ev
+        plain_counts[i] = e.fire_count()
+        e.close()
+    torch.cuda.synchronize()
+    ev0 = sum(eb.info().events_total for _, eb, _ in engines)
+    t0 = time.perf_counter()
+    for _, eb, _ in engines:
+        eb.run_async(steps)
+    for _, eb, _ in engines:
+        eb.sync()
+    ms_b = 1e3 * (time.perf_counter() - t0)
+    ev_b = sum(eb.info().events_total for _, eb, _ in engines) - ev0
+    same = True
+    n_neurons = n_syn = 0
+    cyc = fb = tc = 0
+    err = act = 0.0
+    for idx, eb, _ in engines:
+        fc = eb.fire_count()
+        off = 0
+        for i in idx:
+            n = specs[i].n_pop * specs[i].pop_size
+            same &= bool(np.array_equal(fc[off:off + n], plain_counts[i]))
+            off += n
+        inf = eb.info()
+        n_neurons += inf.n_neurons
+        n_syn += inf.n_synapses
+        st = eb.predictor_stats()
+        cyc += st.cycles
+        fb += st.fallbacks
+        tc += st.tile_cycles
+        err += st.abs_err_sum
+        act += st.actual_sum
+        eb.close()
+    tune = engines[0][2]
+
+    class _St:
+        pass
+    st = _St()
+    st.cycles, st.fallbacks, st.tile_cycles, st.abs_err_sum, st.actual_sum = cyc, fb, tc, err, act
+
+    class _Inf:
+        pass
+    info = _Inf()
+    info.n_neurons, info.n_synapses = n_neurons, n_syn
+    plain = plain_ev / (plain_ms / 1e3)
+    batched = ev_b / (ms_b / 1e3)
+    return {"workload": "%d networks of the batched generator (seed 7), %d cycles each after %d warm-up cycles"
+                        % (n_nets, steps, warm),
+            "neurons": int(info.n_neurons), "synapses": int(info.n_synapses),
+            "plain_events_per_s": plain, "batched_predicted_events_per_s": batched, "ratio": batched / plain,
+            "plain_realtime_factor": steps * 1e-4 * n_nets / (plain_ms / 1e3),
+            "batched_realtime_factor": steps * 1e-4 / (ms_b / 1e3),
+            "batched_engines": len(engines), "batched_timing": "wall clock around all engines' cycles",
+            "spike_counts_identical": same,
+            "predictor": {"train_loss": loss, "train_seconds": t_train, "cycles": st.cycles,
+                          "fallbacks": st.fallbacks, "tile_cycles": st.tile_cycles,
+                          "rel_count_error": st.abs_err_sum / max(st.actual_sum, 1.0)},
+            "autotune": {"delivery": tune.delivery, "block": tune.block_threads, "grid": tune.grid_blocks,
+                         "ns_per_event_push": tune.cost_push[1], "ns_per_event_tile": tune.cost_tile[1]}}
+
+
+# ---------------------------------------------------------------------------
 # Our arm
 # ---------------------------------------------------------------------------
 def main():
@@ -219,6 +340,9 @@ def main():
     ap.add_argument("--settle", type=int, default=1000,
                     help="untimed cycles run at set-up so the network leaves its start-up transient")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batched-nets", type=int, default=32,
+                    help="networks in the batched+predicted vs plain comparison (0 skips it)")
+    ap.add_argument("--batched-steps", type=int, default=1000)
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
@@ -339,6 +463,13 @@ def main():
         except Exception as ex:
             cpu = {"value": None, "unit": "events/s", "cores": 1, "kind": "unavailable", "sample": str(ex)}
 
+    cmp = None
+    if rank == 0 and world == 1 and args.batched_nets > 0:
+        try:
+            cmp = batched_vs_plain(args.batched_nets, args.batched_steps, local)
+        except Exception as ex:
+            cmp = {"error": str(ex)}
+
     if rank == 0:
         line = {"metric": "synaptic events/s", "value": value, "unit": "events/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
@@ -353,7 +484,7 @@ def main():
                 "events_per_step": events_all / args.steps / world,
                 "mean_rate_hz": spikes_all / n_all / (args.steps * DT),
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
-                "gpu_launches": args.steps}
+                "gpu_launches": args.steps, "batched_predicted_vs_plain": cmp}
         print(json.dumps(line))
     eng.close()
     if dist:

@@ -1734,8 +1734,13 @@ int bsim_autotune(bsim_engine *eh, int32_t trial_steps, bsim_tune_result *out)
     cudaEventDestroy(ev1);
     e.block = best_b;
     e.grid = best_g;
-    e.a.delivery = best_m;
-    e.opt.delivery = best_m;
+    // an AUTO engine keeps choosing per cycle; a fixed one takes the fastest mode
+    if (saved_del == BSIM_DELIVERY_AUTO) {
+        e.a.delivery = BSIM_DELIVERY_AUTO;
+    } else {
+        e.a.delivery = best_m;
+        e.opt.delivery = best_m;
+    }
     drop_graph(e);
     out->block_threads = best_b;
     out->grid_blocks = best_g;
@@ -1746,7 +1751,6 @@ int bsim_autotune(bsim_engine *eh, int32_t trial_steps, bsim_tune_result *out)
         out->cost_push[1] = 1e3f * mode_best[BSIM_DELIVERY_PUSH] / (float)mode_ev[BSIM_DELIVERY_PUSH];
     if (mode_best[BSIM_DELIVERY_TILE] < 1e29f && mode_ev[BSIM_DELIVERY_TILE] > 0)
         out->cost_tile[1] = 1e3f * mode_best[BSIM_DELIVERY_TILE] / (float)mode_ev[BSIM_DELIVERY_TILE];
-    (void)saved_del;
     return BSIM_OK;
 }
 

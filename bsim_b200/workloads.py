@@ -66,6 +66,16 @@ def batched(n_nets=256, seed=1):
     return specs, 10000
 
 
+def predicted_2m(seed=1):
+    """200 populations x 10,000 neurons (2e6 neurons, ~2.4e9 synapses), delays U{1..20}, 2 s,
+    i_offset under a 10 Hz square wave (x60 in the odd 50 ms half periods) so population
+    rates swing between tens of Hz and ~1 kHz."""
+    sp = cuba(200, 10000, 500, 20, seed, i_max=0.8e-9)
+    sp.drive_scale = 60.0
+    sp.drive_half_period = 500
+    return [sp], 20000
+
+
 def scaled(spec, pop_size):
     """The same generator with smaller populations (scaled-down replica for CPU checks)."""
     s = cuba(spec.n_pop, pop_size, 100, spec.max_delay, spec.seed)
