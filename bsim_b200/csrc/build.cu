@@ -130,8 +130,8 @@ static uint32_t f2u(float f)
 
 static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab);
 static bool wants_tiles(const bsim_options &o, int32_t D);
-static int build_tiles_host(Engine &e, const int32_t *inst, const int32_t *src, const int32_t *dst,
-                            const float *weight, const int32_t *delay, int64_t s);
+static int build_tiles_host(Engine &e, const int32_t *inst, const int32_t *pop, const int32_t *src,
+                            const int32_t *dst, const float *weight, const int32_t *delay, int64_t s);
 
 static int init_device(Engine &e, const bsim_options *opt)
 {
@@ -336,7 +336,7 @@ static int create_from_arrays(const float *params, int64_t n, const int32_t *pop
         return fail(BSIM_ERR_CUDA, std::string("bsim_create upload: ") + cudaGetErrorString(st));
     }
     if (wants_tiles(e->opt, D)) {
-        rc = build_tiles_host(*e, inst, src, dst, weight, delay, s);
+        rc = build_tiles_host(*e, inst, pop, src, dst, weight, delay, s);
         if (rc != BSIM_OK) {
             free_engine(e);
             return rc;
@@ -436,13 +436,14 @@ static int plan_tiles(const std::vector<int64_t> &run_beg, int64_t tile, std::ve
     return BSIM_OK;
 }
 
-// 32 bytes of shared counters per target: tiles of <= 2048 targets let two
-// 512-thread blocks share an SM.
+// 16 bytes of shared counters per target (four u32 limbs, one sign): tiles of
+// <= 6144 targets let two 512-thread blocks share an SM; large populations are
+// split into equal tiles, small networks into enough tiles to fill the GPU.
 static int64_t auto_tile_size(const bsim_options &o, int64_t N, int sm_count)
 {
-    if (o.tile_size > 0) return std::min<int64_t>(o.tile_size, 4096);
-    int64_t t = (N + 2 * sm_count - 1) / (2 * sm_count);
-    return std::max<int64_t>(256, std::min<int64_t>(2048, t));
+    if (o.tile_size > 0) return std::min<int64_t>(o.tile_size, 12288);
+    int64_t t = (N + sm_count - 1) / sm_count;
+    return std::max<int64_t>(256, std::min<int64_t>(6144, t));
 }
 
 static bool wants_tiles(const bsim_options &o, int32_t D)
@@ -453,6 +454,7 @@ static bool wants_tiles(const bsim_options &o, int32_t D)
 
 // Host-side description of the tiled copy.
 struct TileHost {
+    int32_t n_u = 0;  // target ranges; signed tile q covers range q % n_u with sign q / n_u
     std::vector<int32_t> tile_beg, tile_run_off, tile_units, run_n, run_unit0;
     std::vector<float> tile_scale;
     std::vector<uint32_t> run_src0;
@@ -483,7 +485,7 @@ static int upload_tiles(Engine &e, const TileHost &th)
     float *d_ts;
     uint32_t *d_rs;
     int64_t *d_rp;
-    TRY(dalloc(e, &d_tb, nt + 1));
+    TRY(dalloc(e, &d_tb, th.n_u + 1));
     TRY(dalloc(e, &d_ts, nt));
     TRY(dalloc(e, &d_tro, nt + 1));
     TRY(dalloc(e, &d_tu, nt));
@@ -491,7 +493,7 @@ static int upload_tiles(Engine &e, const TileHost &th)
     TRY(dalloc(e, &d_rn, nr));
     TRY(dalloc(e, &d_rp, nr));
     TRY(dalloc(e, &d_ru, nr));
-    CK(cudaMemcpy(d_tb, th.tile_beg.data(), 4 * (nt + 1), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_tb, th.tile_beg.data(), 4 * (th.n_u + 1), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d_ts, th.tile_scale.data(), 4 * nt, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d_tro, th.tile_run_off.data(), 4 * (nt + 1), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d_tu, th.tile_units.data(), 4 * nt, cudaMemcpyHostToDevice));
@@ -502,6 +504,7 @@ static int upload_tiles(Engine &e, const TileHost &th)
         CK(cudaMemcpy(d_ru, th.run_unit0.data(), 4 * nr, cudaMemcpyHostToDevice));
     }
     a.n_tiles = nt;
+    a.n_tiles_u = th.n_u;
     a.tile_max = th.tile_max;
     a.tile_beg = d_tb;
     a.tile_scale = d_ts;
@@ -514,11 +517,12 @@ static int upload_tiles(Engine &e, const TileHost &th)
     return BSIM_OK;
 }
 
-// Host construction of the tiled copy: synapses sorted by (tile of target,
-// source, delay); one pair per distinct (tile, source), runs of consecutive
-// sources.
-static int build_tiles_host(Engine &e, const int32_t *inst, const int32_t *src, const int32_t *dst,
-                            const float *weight, const int32_t *delay, int64_t s)
+// Host construction of the tiled copy: target ranges follow population (and
+// network) boundaries; synapses sorted by (sign, range of the target, source,
+// delay); one pair per distinct (signed tile, source), runs of consecutive
+// sources. Excitatory tiles come first (they carry most of the synapses).
+static int build_tiles_host(Engine &e, const int32_t *inst, const int32_t *pop, const int32_t *src,
+                            const int32_t *dst, const float *weight, const int32_t *delay, int64_t s)
 {
     const int64_t n = e.N;
     const int32_t D = e.D;
@@ -527,22 +531,25 @@ static int build_tiles_host(Engine &e, const int32_t *inst, const int32_t *src, 
         if (++indeg[dst[k]] > 65535) return fail(BSIM_ERR_LIMIT, "tiled delivery: a neuron has more than 65535 synapses in");
     std::vector<int64_t> runs = {0};
     for (int64_t i = 1; i < n; i++)
-        if (inst && inst[i] != inst[i - 1]) runs.push_back(i);
+        if ((inst && inst[i] != inst[i - 1]) || (pop && pop[i] != pop[i - 1])) runs.push_back(i);
     runs.push_back(n);
     TileHost th;
     plan_tiles(runs, auto_tile_size(e.opt, n, e.sm_count), th.tile_beg, th.tile_max);
-    const int32_t nt = (int32_t)th.tile_beg.size() - 1;
+    th.n_u = (int32_t)th.tile_beg.size() - 1;
+    const int32_t nu = th.n_u, nt = 2 * nu;
     std::vector<int32_t> tile_of(n);
-    for (int32_t q = 0; q < nt; q++)
+    for (int32_t q = 0; q < nu; q++)
         for (int64_t i = th.tile_beg[q]; i < th.tile_beg[q + 1]; i++) tile_of[i] = q;
+    // signed tile (<= 2^27) | source (< 2^31) | delay - 1 (< 64)
     std::vector<std::pair<uint64_t, int64_t>> key(s);
-    for (int64_t k = 0; k < s; k++)
-        key[k] = {((uint64_t)tile_of[dst[k]] << 37) | ((uint64_t)src[k] << 6) | (uint64_t)(delay[k] - 1), k};
+    for (int64_t k = 0; k < s; k++) {
+        const uint64_t q = (uint64_t)(weight[k] >= 0.0f ? 0 : nu) + (uint64_t)tile_of[dst[k]];
+        key[k] = {(q << 37) | ((uint64_t)src[k] << 6) | (uint64_t)(delay[k] - 1), k};
+    }
     std::sort(key.begin(), key.end());
     th.tile_scale.resize(nt);
-    for (int32_t q = 0; q < nt; q++) th.tile_scale[q] = ldexpf(1.0f, e.qexp[inst ? inst[th.tile_beg[q]] : 0]);
+    for (int32_t q = 0; q < nt; q++) th.tile_scale[q] = ldexpf(1.0f, e.qexp[inst ? inst[th.tile_beg[q % nu]] : 0]);
     th.tile_run_off.assign(nt + 1, 0);
-    th.tile_units.assign(0, 0);
     std::vector<int64_t> pair_base;
     std::vector<uint16_t> pair_doff;
     std::vector<uint16_t> ent_tgt(s);
@@ -570,7 +577,7 @@ static int build_tiles_host(Engine &e, const int32_t *inst, const int32_t *src, 
     };
     for (int64_t pos = 0; pos < s; pos++) {
         const int64_t k = key[pos].second;
-        const int32_t q = tile_of[dst[k]];
+        const int32_t q = (int32_t)(key[pos].first >> 37);
         if (q != cur_tile || src[k] != cur_src) {
             if (cur_src >= 0) close_pair();
             const bool extends = q == cur_tile && src[k] == cur_src + 1;
@@ -585,7 +592,7 @@ static int build_tiles_host(Engine &e, const int32_t *inst, const int32_t *src, 
             pair_base.push_back(pos);
         }
         cnt[delay[k] - 1]++;
-        ent_tgt[pos] = (uint16_t)(dst[k] - th.tile_beg[q]);
+        ent_tgt[pos] = (uint16_t)(dst[k] - th.tile_beg[q % nu]);
         ent_w[pos] = weight[k];
     }
     if (cur_src >= 0) {
@@ -799,7 +806,7 @@ struct TileSeg {
     uint32_t p24, exc24;
     float w_exc, w_inh;
     int32_t d_inst;     // the network's max delay
-    int32_t pad;
+    int32_t sign;       // 0: excitatory synapses only (w >= 0), 1: inhibitory only
 };
 
 static __device__ __forceinline__ int find_seg(const TileSeg *segs, int n_segs, int64_t k)
@@ -833,8 +840,9 @@ __global__ void gen_tile_kernel(const TileSeg *segs, int n_segs, int64_t n_pairs
         for (int j0 = sg.j0; j0 < sg.j1; j0 += 32) {
             const int j = j0 + lane;
             SynDraw sd;
-            const bool conn = j < sg.j1 && draw_pair(sg.pseed, (uint64_t)i, (uint64_t)j, sg.p24, sg.exc24, sg.w_exc,
-                                                     sg.w_inh, sg.d_inst, &sd);
+            bool conn = j < sg.j1 && draw_pair(sg.pseed, (uint64_t)i, (uint64_t)j, sg.p24, sg.exc24, sg.w_exc,
+                                               sg.w_inh, sg.d_inst, &sd);
+            if (conn) conn = (sd.w >= 0.0f) == (sg.sign == 0);
             if (!__ballot_sync(0xffffffffu, conn)) continue;
             const unsigned same = __match_any_sync(0xffffffffu, conn ? sd.d : -1);
             if (conn) {
@@ -1080,29 +1088,33 @@ static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, co
     const bool tiles = wants_tiles(E.opt, D) &&
                        *std::max_element(maxdeg.begin(), maxdeg.end()) <= 65535ull;
     if (tiles) {
+        // target ranges follow population boundaries
         std::vector<int64_t> runs;
-        for (int k = 0; k < ns; k++) runs.push_back(gi[k].nbase);
+        for (int k = 0; k < ns; k++)
+            for (int pp = 0; pp < gi[k].P; pp++) runs.push_back(gi[k].nbase + (int64_t)pp * gi[k].n);
         runs.push_back(N);
         std::vector<int32_t> tile_beg;
         int32_t tile_max = 0;
         plan_tiles(runs, auto_tile_size(E.opt, N, E.sm_count), tile_beg, tile_max);
-        const int32_t nt = (int32_t)tile_beg.size() - 1;
+        const int32_t nu = (int32_t)tile_beg.size() - 1, nt = 2 * nu;
         std::vector<TileSeg> segs;
         TileHost th;
+        th.n_u = nu;
         th.tile_beg = tile_beg;
         th.tile_max = tile_max;
         th.tile_scale.resize(nt);
         th.tile_run_off.assign(nt + 1, 0);
         int64_t pairs = 0;
-        int k = 0;
         for (int32_t q = 0; q < nt; q++) {
-            while (k + 1 < ns && gi[k + 1].nbase <= tile_beg[q]) k++;
+            const int32_t qu = q % nu, sign = q / nu;
+            int k = 0;
+            while (k + 1 < ns && gi[k + 1].nbase <= tile_beg[qu]) k++;
             const GenInst &x = gi[k];
             const GenPlan &pl = plans[k];
             th.tile_units.push_back(0);
             th.tile_run_off[q + 1] = th.tile_run_off[q];
             th.tile_scale[q] = ldexpf(1.0f, E.qexp[k]);
-            const int64_t lb = tile_beg[q] - x.nbase, le = tile_beg[q + 1] - x.nbase;
+            const int64_t lb = tile_beg[qu] - x.nbase, le = tile_beg[qu + 1] - x.nbase;
             for (int64_t pp = lb / x.n; pp <= (le - 1) / x.n; pp++) {
                 const int64_t pop_beg = pp * x.n;
                 const int32_t j0 = (int32_t)(std::max(lb, pop_beg) - pop_beg);
@@ -1121,7 +1133,7 @@ static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, co
                     sg.w_exc = x.w_exc;
                     sg.w_inh = x.w_inh;
                     sg.d_inst = x.D;
-                    sg.pad = 0;
+                    sg.sign = sign;
                     segs.push_back(sg);
                     add_run(th, (uint32_t)sg.src_base, x.n, pairs, D);
                     pairs += x.n;

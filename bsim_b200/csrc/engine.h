@@ -73,13 +73,17 @@ struct StepArgs {
     // per-population spike counts of the last hist_len steps (predictor input)
     int32_t *pop_hist;          // [hist_len][n_pops]
     int32_t n_pops, hist_len;
-    // target-tiled delivery (BSIM_DELIVERY_TILE). A tile's sources form runs of
-    // consecutive neuron ids; every source of a run owns one (tile, source) pair.
-    int32_t n_tiles;
-    int32_t tile_max;                // largest tile (neurons): shared-memory accumulator size
-    const int32_t *tile_beg;         // [n_tiles + 1] first target of each tile
+    // target-tiled delivery (BSIM_DELIVERY_TILE). Target ranges ("tiles") are
+    // summed separately for excitatory and inhibitory synapses: signed tile q
+    // covers range q % n_tiles_u with sign q / n_tiles_u (0: E, 1: I). A signed
+    // tile's sources form runs of consecutive neuron ids; every source of a run
+    // owns one (signed tile, source) pair.
+    int32_t n_tiles;                 // signed tiles = 2 * n_tiles_u (0: no tiled copy)
+    int32_t n_tiles_u;               // target ranges
+    int32_t tile_max;                // largest range (neurons): shared-memory accumulator size
+    const int32_t *tile_beg;         // [n_tiles_u + 1] first target of each range
     const float *tile_scale;         // [n_tiles] 2^qexp of the tile's network
-    const int32_t *tile_run_off;     // [n_tiles + 1] range of runs
+    const int32_t *tile_run_off;     // [n_tiles + 1] range of runs (signed tiles)
     const int32_t *tile_units;       // [n_tiles] work units: sum over runs of ceil(n/32) * D
     const uint32_t *run_src0;        // [runs] first source
     const int32_t *run_n;            // [runs] sources in the run

@@ -346,9 +346,12 @@ static __device__ __forceinline__ unsigned long long pull_phase(const StepArgs &
 }
 
 // ---------------------------------------------------------------------------
-// Phase B, tiled: each block owns a contiguous tile of target neurons and sums
-// their input exactly in shared memory, so no global atomic is issued; the
-// tile is written out once at the end.
+// Phase B, tiled: each block owns a contiguous tile of target neurons and one
+// sign (the excitatory or the inhibitory synapses into it) and sums those
+// inputs exactly in shared memory, so no global atomic is issued; the tile's
+// half of each {E, I} accumulator pair is written out once at the end. Tiles
+// follow population boundaries and hold up to a few thousand targets (16 bytes
+// of counters each), so each source's row into a tile stays a long segment.
 //
 // The tile's synapses are grouped by (source, delay) and its sources form runs
 // of consecutive ids. A work unit is (run, delay d, 32-source chunk): one lane
@@ -365,7 +368,7 @@ static __device__ __forceinline__ unsigned long long pull_phase(const StepArgs &
 // ---------------------------------------------------------------------------
 #define TILE_SEGS 64
 
-// Counters are limb-major ([4][2 * tile]: limb k of sum i at k * stride + i) so
+// Counters are limb-major ([4][tile]: limb k of target i at k * stride + i) so
 // that lanes adding into scattered targets spread over all shared-memory banks.
 static __device__ __forceinline__ void limb_add(unsigned *c, int stride, long long v)
 {
@@ -393,8 +396,9 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
     int *seg_cum = s_cum + warp * TILE_SEGS;
     unsigned long long ev = 0;
     for (int q = blockIdx.x; q < a.n_tiles; q += gridDim.x) {
-        const int tb = a.tile_beg[q], T = a.tile_beg[q + 1] - tb;
-        for (int i = threadIdx.x; i < 8 * T; i += blockDim.x) s_acc[i] = 0u;
+        const int qu = q % a.n_tiles_u, sign = q / a.n_tiles_u;
+        const int tb = a.tile_beg[qu], T = a.tile_beg[qu + 1] - tb;
+        for (int i = threadIdx.x; i < 4 * T; i += blockDim.x) s_acc[i] = 0u;
         __syncthreads();
         const float sc = a.tile_scale[q];
         const int r0 = a.tile_run_off[q], r1 = a.tile_run_off[q + 1];
@@ -483,7 +487,7 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
                     for (int uu = 0; uu < 4; uu++) {
                         if (f0 + uu * 32 + lane < n_ent) {
                             const long long qv = __float2ll_rn(__fmul_rn(wv[uu], sc));
-                            limb_add(s_acc + 2 * (int)tg[uu] + (wv[uu] >= 0.0f ? 0 : 1), 2 * T, qv);
+                            limb_add(s_acc + (int)tg[uu], T, qv);
                         }
                     }
                 }
@@ -491,9 +495,9 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
             }
         }
         __syncthreads();
-        longlong2 *g = reinterpret_cast<longlong2 *>(a.acc) + (int64_t)pw * a.N + tb;
-        for (int i = threadIdx.x; i < T; i += blockDim.x)
-            g[i] = make_longlong2(limb_sum(s_acc + 2 * i, 2 * T), limb_sum(s_acc + 2 * i + 1, 2 * T));
+        // this tile's sign half of each target's {E, I} accumulator pair
+        long long *g = reinterpret_cast<long long *>(a.acc) + 2 * ((int64_t)pw * a.N + tb) + sign;
+        for (int i = threadIdx.x; i < T; i += blockDim.x) g[2 * i] = limb_sum(s_acc + i, T);
         __syncthreads();
     }
     return ev;
@@ -617,7 +621,7 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const StepAr
     __shared__ PushSeg s_seg[MAX_WARPS * PUSH_CHUNK];
     __shared__ int s_wcnt[64];
     __shared__ unsigned long long s_ev;
-    // tiled delivery: [4][2 * tile] u32 limb counters, then per-warp segment lists
+    // tiled delivery: [4][tile] u32 limb counters (one sign), then per-warp segment lists
     extern __shared__ __align__(16) unsigned long long s_dyn[];
     const unsigned long long t = *reinterpret_cast<volatile unsigned long long *>(a.step_ctr);
     const int p = (int)(t & 1ull);
@@ -649,7 +653,7 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const StepAr
     if (push) {
         ev = push_phase(a, t, p ^ 1, s_cum, s_seg);
     } else if (tiled) {
-        long long *starts = reinterpret_cast<long long *>(s_dyn + 4 * a.tile_max);
+        long long *starts = reinterpret_cast<long long *>(s_dyn + 2 * a.tile_max);
         int *cums = reinterpret_cast<int *>(starts + MAX_WARPS * TILE_SEGS);
         ev = tile_phase(a, t, p ^ 1, reinterpret_cast<unsigned *>(s_dyn), starts, cums);
     } else {
@@ -709,7 +713,7 @@ __global__ void record_flush_kernel(const StepArgs a)
 size_t step_dynamic_smem(const StepArgs &a)
 {
     if (a.n_tiles == 0) return 0;
-    return (size_t)8 * a.tile_max * sizeof(unsigned) + (size_t)MAX_WARPS * TILE_SEGS * (sizeof(long long) + sizeof(int));
+    return (size_t)4 * a.tile_max * sizeof(unsigned) + (size_t)MAX_WARPS * TILE_SEGS * (sizeof(long long) + sizeof(int));
 }
 
 // The attribute belongs to the kernel, not to an engine: it only ever grows,
