@@ -132,6 +132,20 @@ def profiled_traffic(config):
     return None
 
 
+def reduce_over_ranks(dist, maxes, sums, device="cpu"):
+    """Max over ranks of each value in `maxes` and sum over ranks of each value in
+    `sums` (float64). With dist None (one process) the values come back unchanged.
+    Every rank must call it with the same number of values."""
+    import torch
+    if dist is None:
+        return [float(v) for v in maxes], [float(v) for v in sums]
+    mx = torch.tensor([float(v) for v in maxes], dtype=torch.float64, device=device)
+    sm = torch.tensor([float(v) for v in sums], dtype=torch.float64, device=device)
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return mx.tolist(), sm.tolist()
+
+
 # ---------------------------------------------------------------------------
 # CPU baselines (oracle/_ref: the reference's own simulator, else the oracle port)
 # ---------------------------------------------------------------------------
@@ -158,8 +172,8 @@ def cpu_baseline(spec, steps, budget_s=20.0):
     import netio
     S_full = spec.n_pop * (spec.pop_size ** 2) * spec.p_conn * 1.2
     ref = oracle.ref_available("f32")
-    # the reference walks every synapse every step (~20 ns each on one core)
-    pop = int(spec.pop_size * min(1.0, np.sqrt(budget_s / (20e-9 * S_full * steps))))
+    # the reference walks every synapse every step (~60 ns each on one core at these rates)
+    pop = int(spec.pop_size * min(1.0, np.sqrt(budget_s / (60e-9 * S_full * steps))))
     pop = max(pop, 20)
     rs, g, net = replica_net(spec, pop)
     orc = oracle.run(g["params"], g["src"], g["dst"], g["weight"], g["delay_steps"], np.float32(DT), steps)
@@ -392,15 +406,7 @@ def main():
     i1 = eng.info()
     events = int(i1.events_total - i0.events_total)
     spikes = int((eng.fire_count().astype(np.int64) - fc0).sum())
-    tot = torch.tensor([ms, float(events), float(spikes), float(N)], dtype=torch.float64, device="cuda")
-    if dist:
-        mx = tot.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = tot.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        ms_max, events_all, spikes_all, n_all = float(mx[0]), float(sm[1]), float(sm[2]), float(sm[3])
-    else:
-        ms_max, events_all, spikes_all, n_all = ms, float(events), float(spikes), float(N)
+    (ms_max,), (events_all, spikes_all, n_all) = reduce_over_ranks(dist, [ms], [events, spikes, N], "cuda")
     value = events_all / (ms_max / 1e3)
     rtf = args.steps * DT / (ms_max / 1e3)
     ms_step = ms_max / args.steps
@@ -427,15 +433,7 @@ def main():
     ib = eng.info()
     ev_e2e = float(ib.events_total - ia.events_total)
     spk_e2e = sum(len(r) for r in raster)
-    t_e2e_max = t_e2e
-    ev_all_e2e = ev_e2e
-    if dist:
-        x = torch.tensor([t_e2e, ev_e2e], dtype=torch.float64, device="cuda")
-        mx = x.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = x.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        t_e2e_max, ev_all_e2e = float(mx[0]), float(sm[1])
+    (t_e2e_max,), (ev_all_e2e,) = reduce_over_ranks(dist, [t_e2e], [ev_e2e], "cuda")
     e2e = {"value": ev_all_e2e / t_e2e_max, "unit": "events/s",
            "h2d_bytes_per_step": 16.0 * N / e2e_steps,
            "d2h_bytes_per_step": (4.0 * spk_e2e + 8.0 * (e2e_steps + 1) + 4.0 * len(counts)) / e2e_steps,

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_segmented_sort.cuh>
 
 #include "engine.h"
 #include "netgen.h"
@@ -1419,8 +1420,33 @@ int bsim_read_raster(bsim_engine *eh, int64_t *step_off, int32_t *ids, int64_t i
     if (total > ctl.cap) return fail(BSIM_ERR_LIMIT, "raster buffer overflowed");
     if (ids) {
         if (total > ids_cap) return fail(BSIM_ERR_ARG, "bsim_read_raster: ids buffer too small");
-        CK(cudaMemcpy(ids, e.a.rec_ids, sizeof(int32_t) * total, cudaMemcpyDeviceToHost));
-        for (int64_t k = 0; k < ns; k++) std::sort(ids + step_off[k], ids + step_off[k + 1]);
+        if (total == 0) return BSIM_OK;
+        // ascending ids within each cycle: one segmented sort on the device (the
+        // cycles' segments tile the recording); recordings of 2^31 ids or more
+        // are sorted on the host
+        if (total >= ((int64_t)1 << 31) || ns >= ((int64_t)1 << 31)) {
+            CK(cudaMemcpy(ids, e.a.rec_ids, sizeof(int32_t) * total, cudaMemcpyDeviceToHost));
+            for (int64_t k = 0; k < ns; k++) std::sort(ids + step_off[k], ids + step_off[k + 1]);
+            return BSIM_OK;
+        }
+        int32_t *d_sorted = nullptr;
+        void *d_tmp = nullptr;
+        size_t tmp_bytes = 0;
+        cudaError_t st = cub::DeviceSegmentedSort::SortKeys(nullptr, tmp_bytes, e.a.rec_ids, d_sorted, (int)total,
+                                                            (int)ns, e.a.rec_off, e.a.rec_off + 1, e.stream);
+        if (st == cudaSuccess) st = cudaMalloc((void **)&d_sorted, sizeof(int32_t) * total);
+        if (st == cudaSuccess) st = cudaMalloc(&d_tmp, tmp_bytes ? tmp_bytes : 1);
+        if (st == cudaSuccess)
+            st = cub::DeviceSegmentedSort::SortKeys(d_tmp, tmp_bytes, e.a.rec_ids, d_sorted, (int)total, (int)ns,
+                                                    e.a.rec_off, e.a.rec_off + 1, e.stream);
+        if (st == cudaSuccess) st = cudaMemcpyAsync(ids, d_sorted, sizeof(int32_t) * total, cudaMemcpyDeviceToHost, e.stream);
+        if (st == cudaSuccess) st = cudaStreamSynchronize(e.stream);
+        cudaFree(d_tmp);
+        cudaFree(d_sorted);
+        if (st != cudaSuccess) {
+            cudaGetLastError();
+            return fail(BSIM_ERR_CUDA, std::string("bsim_read_raster: ") + cudaGetErrorString(st));
+        }
     }
     return BSIM_OK;
 }
