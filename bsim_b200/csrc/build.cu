@@ -1556,7 +1556,8 @@ __global__ void pop_degree_tiles_kernel(StepArgs a, double *in_sum, double *out_
                 const double c = (double)a.pair_doff[k * (a.D + 1) + a.D];
                 const uint32_t src = a.run_src0[r] + i;
                 if (want_out) atomicAdd(&out_sum[a.ctab[a.cls[src]].pop], c);
-                if (want_in) atomicAdd(&in_sum[a.ctab[a.cls[a.tile_beg[q]]].pop], c);
+                // tile_beg is indexed by target range: signed tile q covers range q % n_tiles_u
+                if (want_in) atomicAdd(&in_sum[a.ctab[a.cls[a.tile_beg[q % a.n_tiles_u]]].pop], c);
             }
         }
     }

@@ -121,3 +121,25 @@ def test_autotune_keeps_dynamics(trained):
     a.run(300)
     b.run(300)
     assert np.array_equal(a.state()["v"], b.state()["v"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("opts", [dict(delivery=B.DELIVERY_AUTO), dict(delivery=B.DELIVERY_TILE),
+                                  dict(), dict(delivery=B.DELIVERY_PULL)])
+def test_population_degrees_from_every_synapse_copy(opts):
+    """Mean in/out-degree per population as the engine derives them (from the
+    pull rows, the push rows or the tiled copy, whichever it holds) against the
+    host generator's synapse list, for two networks packed in one engine."""
+    specs = [W.cuba(4, 300, 100, 6, seed=61), W.cuba(3, 400, 500, 12, seed=62)]
+    eng = B.Engine.generated(specs, DT, opts=B.options(**opts))
+    size, indeg, outdeg = eng.pop_info()
+    want_in, want_out, want_size = [], [], []
+    for sp in specs:
+        g = B.gen_host(sp)
+        pops = g["pop"]
+        P = sp.n_pop
+        want_size += [sp.pop_size] * P
+        want_in += list(np.bincount(pops[g["dst"]], minlength=P) / sp.pop_size)
+        want_out += list(np.bincount(pops[g["src"]], minlength=P) / sp.pop_size)
+    assert list(size) == want_size
+    assert np.allclose(indeg, want_in, rtol=1e-6) and np.allclose(outdeg, want_out, rtol=1e-6)
