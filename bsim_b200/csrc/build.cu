@@ -1546,6 +1546,20 @@ __global__ void pop_degree_kernel(StepArgs a, int32_t *size, double *in_sum, dou
     }
 }
 
+// In-degree of every neuron from the push rows (when no target-ordered copy exists).
+__global__ void indeg_from_push_kernel(StepArgs a, int32_t *indeg)
+{
+    const int64_t S = a.row_off[a.N * a.D];
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < S; k += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(&indeg[a.syn[k].x], 1);
+}
+
+__global__ void pop_in_from_counts_kernel(StepArgs a, const int32_t *indeg, double *in_sum)
+{
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < a.N; j += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(&in_sum[a.ctab[a.cls[j]].pop], (double)indeg[j]);
+}
+
 __global__ void pop_degree_tiles_kernel(StepArgs a, double *in_sum, double *out_sum, int want_in, int want_out)
 {
     // one block per tile: entries per pair give out-degree of the source and in-degree of the tile
@@ -1579,8 +1593,20 @@ static int ensure_pop_info(Engine &e)
     CK(cudaMemset(d_in, 0, 8 * P));
     CK(cudaMemset(d_out, 0, 8 * P));
     pop_degree_kernel<<<e.sm_count * 4, 256, 0, e.stream>>>(e.a, d_size, d_in, d_out);
-    if (e.a.n_tiles > 0 && (!e.a.col_off || !e.a.row_off))
-        pop_degree_tiles_kernel<<<e.sm_count * 4, 256, 0, e.stream>>>(e.a, d_in, d_out, e.a.col_off ? 0 : 1,
+    bool in_done = e.a.col_off != nullptr;
+    if (!in_done && e.a.row_off) {
+        int32_t *d_indeg = nullptr;
+        CK(cudaMalloc((void **)&d_indeg, sizeof(int32_t) * e.N));
+        cudaMemsetAsync(d_indeg, 0, sizeof(int32_t) * e.N, e.stream);
+        indeg_from_push_kernel<<<e.sm_count * 8, 256, 0, e.stream>>>(e.a, d_indeg);
+        pop_in_from_counts_kernel<<<e.sm_count * 4, 256, 0, e.stream>>>(e.a, d_indeg, d_in);
+        cudaError_t st = cudaStreamSynchronize(e.stream);
+        cudaFree(d_indeg);
+        if (st != cudaSuccess) return fail(BSIM_ERR_CUDA, std::string("population degrees: ") + cudaGetErrorString(st));
+        in_done = true;
+    }
+    if (e.a.n_tiles > 0 && (!in_done || !e.a.row_off))
+        pop_degree_tiles_kernel<<<e.sm_count * 4, 256, 0, e.stream>>>(e.a, d_in, d_out, in_done ? 0 : 1,
                                                                       e.a.row_off ? 0 : 1);
     CK(cudaStreamSynchronize(e.stream));
     std::vector<int32_t> sz(P);
