@@ -121,12 +121,13 @@ def measured_hbm_peak():
     return HBM_FALLBACK_GBS, "fallback"
 
 
-def profiled_traffic(config):
-    """DRAM bytes per launch of the step kernel from the committed ncu summary, if any."""
+def profiled_traffic(config, delivery):
+    """DRAM bytes per launch of the step kernel from the committed ncu summaries,
+    keyed by workload and delivery mode ("plain_1m/push"), if one was captured."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(p):
         d = json.load(open(p))
-        v = d.get(config)
+        v = d.get("%s/%s" % (config, delivery))
         if isinstance(v, dict):
             return v.get("bytes_per_launch")
     return None
@@ -445,7 +446,7 @@ def main():
     alg_bytes = (BYTES_PER_NEURON_STEP * N + BYTES_PER_EVENT * events / args.steps +
                  BYTES_PER_SPIKE * spikes / args.steps)
     achieved = alg_bytes / (ms / args.steps / 1e3) / 1e9
-    traffic = profiled_traffic(args.config)
+    traffic = profiled_traffic(args.config, args.delivery)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
             if peak_kind == "measured" else "fallback 6.65 TB/s",
