@@ -23,6 +23,9 @@ DELIVERY_PUSH = 0
 DELIVERY_PULL = 1
 DELIVERY_AUTO = 2
 DELIVERY_TILE = 3
+NEURON_LIF = 0
+NEURON_CONSTANT = 1
+NEURON_POISSON = 2
 MAX_DELAY = 1024
 
 
@@ -62,7 +65,7 @@ class Info(ctypes.Structure):
 
 
 EXPORTS = [
-    "bsim_options_default", "bsim_create", "bsim_create_generated", "bsim_gen_count", "bsim_gen_host",
+    "bsim_options_default", "bsim_create", "bsim_create_mixed", "bsim_create_generated", "bsim_gen_count", "bsim_gen_host",
     "bsim_synapse_reset", "bsim_run", "bsim_run_async", "bsim_sync", "bsim_record", "bsim_read_raster",
     "bsim_read_state", "bsim_read_fire_count", "bsim_read_pop_counts", "bsim_get_info", "bsim_get_qexp",
     "bsim_destroy", "bsim_last_error", "bsim_write_state", "bsim_get_stream", "bsim_set_drive",
@@ -100,6 +103,7 @@ def lib():
         sig = {
             "bsim_options_default": [P],
             "bsim_create": [P, i64, P, P, P, P, P, P, i64, f32, P, P],
+            "bsim_create_mixed": [P, P, i64, P, P, P, P, P, P, i64, f32, ctypes.c_uint64, P, P],
             "bsim_create_generated": [P, i32, f32, P, P],
             "bsim_gen_count": [P, P, P],
             "bsim_gen_host": [P, P, P, P, P, P, P],
@@ -237,7 +241,10 @@ class Engine:
         self._h = handle
 
     @classmethod
-    def from_arrays(cls, params, src, dst, weight, delay_steps, dt, pop=None, instance=None, opts=None):
+    def from_arrays(cls, params, src, dst, weight, delay_steps, dt, pop=None, instance=None, opts=None,
+                    kind=None, input_seed=0):
+        """kind: per-neuron NEURON_LIF / NEURON_CONSTANT / NEURON_POISSON (None: all LIF);
+        input_seed: seed of the Poisson neurons' draws."""
         params = np.ascontiguousarray(params, np.float32)
         src = np.ascontiguousarray(src, np.int32)
         dst = np.ascontiguousarray(dst, np.int32)
@@ -247,8 +254,15 @@ class Engine:
         instance = None if instance is None else np.ascontiguousarray(instance, np.int32)
         opts = opts or options()
         h = ctypes.c_void_p()
-        _check(lib().bsim_create(_p(params), params.shape[0], _p(pop), _p(instance), _p(src), _p(dst), _p(weight),
-                                 _p(delay_steps), src.shape[0], dt, ctypes.byref(opts), ctypes.byref(h)))
+        if kind is None:
+            _check(lib().bsim_create(_p(params), params.shape[0], _p(pop), _p(instance), _p(src), _p(dst),
+                                     _p(weight), _p(delay_steps), src.shape[0], dt, ctypes.byref(opts),
+                                     ctypes.byref(h)))
+        else:
+            kind = np.ascontiguousarray(kind, np.uint8)
+            _check(lib().bsim_create_mixed(_p(params), _p(kind), params.shape[0], _p(pop), _p(instance), _p(src),
+                                           _p(dst), _p(weight), _p(delay_steps), src.shape[0], dt, input_seed,
+                                           ctypes.byref(opts), ctypes.byref(h)))
         return cls(h)
 
     @classmethod

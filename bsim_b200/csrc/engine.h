@@ -7,12 +7,16 @@
 #include <vector>
 
 #include "../../include/bsim_b200.h"
+#include "drive.h"
 
 namespace bsim {
 
-// One folded LIF parameter tuple: the per-population part of LIFENeuron::reset's
-// output (src/neuron/lif/LIFENeuron.cpp:68-112). v_tmp depends on i_offset and is
-// kept per neuron. 48 bytes; the table is small and read through the L1 cache.
+// One neuron class. For LIF_brian neurons: a folded parameter tuple, the
+// per-population part of LIFENeuron::reset's output (src/neuron/lif/LIFENeuron.cpp:68-112);
+// v_tmp depends on i_offset and is kept per neuron. Input-drive neurons
+// (BSIM_NEURON_CONSTANT / _POISSON) keep their parameters per neuron in the state
+// slots and use only kind, pop, inst and id_base here. 64 bytes; the table is small
+// and read through the L1 cache.
 struct ClassParams {
     float Cm, CE, CI, C_E, C_I, v_thresh, v_reset;
     int32_t refrac_time;
@@ -20,6 +24,9 @@ struct ClassParams {
     float scale_down;  // 2^-qexp
     int32_t pop;       // population (spike statistics)
     int32_t inst;      // independent network
+    int32_t kind;      // BSIM_NEURON_*
+    int32_t id_base;   // first neuron id of the network (Poisson draws use id - id_base)
+    int32_t reserved[2];
 };
 
 // Raster recording window: cycles [t0, t0 + steps) into a buffer of cap ids.
@@ -43,10 +50,14 @@ struct StepArgs {
     int32_t R;         // ring slots = D + 2
     int64_t cap;       // fired ids per ring slot
     int64_t W;         // bitmap words per ring slot = ceil(N / 32)
-    float4 *state;     // [N] {v, i_E, i_I, refrac_step as int bits}
-    const float *vtmp; // [N]
+    float4 *state;     // [N] LIF: {v, i_E, i_I, refrac_step as int bits}
+                       //     Constant: {fire_rate, start_cycle, end_cycle, fire_count} (ints as bits)
+                       //     Poisson: {rate, fire_cycle, end_cycle, refrac_step} (ints as bits)
+    const float *vtmp; // [N] LIF: v_tmp; Poisson: exp(-(rate mod 64)); Constant: unused
     const float *vtmp_alt;  // [N] v_tmp of the odd half periods of a square-wave drive (may be NULL)
     int32_t drive_half;     // cycles per half period (0: constant drive)
+    PoissonTables ptab;     // inversion tables of the Poisson sampler (NULL thr: no Poisson neurons)
+    uint64_t input_seed;    // seed of the Poisson neurons' draws
     const uint16_t *cls;       // [N] class of each neuron
     const ClassParams *ctab;   // [n_cls]
     void *acc;                 // [2][N] longlong2 (EXACT) or float2 (ORDERED): input for the next step

@@ -38,6 +38,33 @@ static __device__ __forceinline__ void red_add_u64(unsigned long long *p, unsign
 }
 
 // ---------------------------------------------------------------------------
+// Input-drive neurons (drive.h): Constant_spikes per update_constant_neuron
+// (src/neuron/constant/constant.cu:18-22), Poisson_spikes per update_poisson_neuron
+// and reset_poisson_neuron (src/neuron/poisson/poisson.cu:29-31, 9-15). Both
+// ignore their synaptic input, as their recv() does.
+// ---------------------------------------------------------------------------
+static __device__ __forceinline__ void drive_update(const StepArgs &a, int kind, int64_t j, int t,
+                                                 const ClassParams *c, float4 &st, bool &fired)
+{
+    if (kind == BSIM_NEURON_CONSTANT) {
+        const int cnt = __float_as_int(st.w);
+        if (t < __float_as_int(st.z) && __fmul_rn((float)(t - __float_as_int(st.y)), st.x) > (float)cnt) {
+            fired = true;
+            st.w = __int_as_float(cnt + 1);
+        }
+    } else {
+        const int fc = __float_as_int(st.y);
+        if (t == fc && t <= __float_as_int(st.z)) {
+            fired = true;
+            const uint64_t key = poisson_key(a.input_seed, j - __ldg(&c->id_base), fc);
+            const long long nxt = (long long)fc + 1 + poisson_draw(key, st.x, a.vtmp[j], a.ptab) +
+                                  __float_as_int(st.w);
+            st.y = __int_as_float(nxt > 2147483647LL ? 2147483647 : (int)nxt);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Phase A: LIF_brian update of a grid-stride share of the neurons.
 // Arithmetic follows LIFENeuron::update term by term with every product and
 // sum rounded on its own (no FMA contraction), as the reference's x86 build
@@ -79,27 +106,32 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
                 inE = q.x;
                 inI = q.y;
             }
-            if (refrac > 0) {
-                refrac -= 1;  // input of this cycle is dropped
-            } else {
-                const float Cm = __ldg(&c->Cm), C_E = __ldg(&c->C_E), C_I = __ldg(&c->C_I);
-                float v = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(Cm, st.x), vtmp[j]), __fmul_rn(st.y, C_E)),
-                                    __fmul_rn(st.z, C_I));
-                float iE = __fmul_rn(__ldg(&c->CE), st.y);
-                float iI = __fmul_rn(__ldg(&c->CI), st.z);
-                if (v >= __ldg(&c->v_thresh)) {
-                    fired = true;
-                    refrac = __ldg(&c->refrac_time) - 1;
-                    v = __ldg(&c->v_reset);
+            const int kind = __ldg(&c->kind);
+            if (kind == BSIM_NEURON_LIF) {
+                if (refrac > 0) {
+                    refrac -= 1;  // input of this cycle is dropped
                 } else {
-                    iE = __fadd_rn(iE, inE);
-                    iI = __fadd_rn(iI, inI);
+                    const float Cm = __ldg(&c->Cm), C_E = __ldg(&c->C_E), C_I = __ldg(&c->C_I);
+                    float v = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(Cm, st.x), vtmp[j]), __fmul_rn(st.y, C_E)),
+                                        __fmul_rn(st.z, C_I));
+                    float iE = __fmul_rn(__ldg(&c->CE), st.y);
+                    float iI = __fmul_rn(__ldg(&c->CI), st.z);
+                    if (v >= __ldg(&c->v_thresh)) {
+                        fired = true;
+                        refrac = __ldg(&c->refrac_time) - 1;
+                        v = __ldg(&c->v_reset);
+                    } else {
+                        iE = __fadd_rn(iE, inE);
+                        iI = __fadd_rn(iI, inI);
+                    }
+                    st.x = v;
+                    st.y = iE;
+                    st.z = iI;
                 }
-                st.x = v;
-                st.y = iE;
-                st.z = iI;
+                st.w = __int_as_float(refrac);
+            } else {
+                drive_update(a, kind, j, (int)t, c, st, fired);  // input is dropped (recv returns 0)
             }
-            st.w = __int_as_float(refrac);
             a.state[j] = st;
             if (hist) pop = __ldg(&c->pop);
         }
@@ -615,7 +647,7 @@ static __device__ __forceinline__ void record_phase(const StepArgs &a, unsigned 
 }
 
 template <int ACC>
-__global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const StepArgs a)
+__global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const __grid_constant__ StepArgs a)
 {
     __shared__ long long s_cum[BSIM_MAX_DELAY + 1];
     __shared__ PushSeg s_seg[MAX_WARPS * PUSH_CHUNK];

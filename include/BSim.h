@@ -131,6 +131,53 @@ public:
     virtual Type getType() { return LIFE; }
     const real *params() const { return _p; }
     const static Type type = LIFE;
+    const static uint8_t kind = BSIM_NEURON_LIF;
+
+private:
+    real _p[10];
+};
+
+/* Spikes at a constant rate (src/neuron/constant/ConstantNeuron.h:15-50): fire_rate in
+ * spikes per cycle, active from start_time until end_time (seconds). */
+class ConstantNeuron : public NeuronBase {
+public:
+    ConstantNeuron(real fire_rate, real start_time = 0.0, real end_time = 1.0e9)
+    {
+        memset(_p, 0, sizeof(_p));
+        _p[0] = fire_rate;
+        _p[1] = start_time;
+        _p[2] = end_time;
+    }
+    virtual Type getType() { return Constant; }
+    void setRate(real rate) { _p[0] = rate; }
+    void setStart(real time) { _p[1] = time; }
+    void setEnd(real time) { _p[2] = time; }
+    const real *params() const { return _p; }
+    const static Type type = Constant;
+    const static uint8_t kind = BSIM_NEURON_CONSTANT;
+
+private:
+    real _p[10];
+};
+
+/* Spikes with Poisson-distributed gaps (src/neuron/poisson/PoissonNeuron.h:18-58): rate is
+ * the mean gap in cycles, refract the dead time after a spike (s), active for duration
+ * seconds from start_time. Draws come from the engine's seeded generator
+ * (BSIM_INPUT_SEED in the environment, default 1) instead of the system clock. */
+class PoissonNeuron : public NeuronBase {
+public:
+    PoissonNeuron(real rate, real refract, real start_time = 0, real duration = 1000)
+    {
+        memset(_p, 0, sizeof(_p));
+        _p[0] = rate;
+        _p[1] = refract;
+        _p[2] = start_time;
+        _p[3] = duration;
+    }
+    virtual Type getType() { return Poisson; }
+    const real *params() const { return _p; }
+    const static Type type = Poisson;
+    const static uint8_t kind = BSIM_NEURON_POISSON;
 
 private:
     real _p[10];
@@ -157,6 +204,8 @@ private:
 
 typedef CompositeNeuron<LIFENeuron, StaticSynapse> LIF_brian;
 typedef CompositeNeuron<LIFENeuron, StaticSynapse> IF_curr_exp;
+typedef CompositeNeuron<ConstantNeuron, StaticSynapse> Constant_spikes;  // include/Neuron.h:25
+typedef CompositeNeuron<PoissonNeuron, StaticSynapse> Poisson_spikes;    // include/Neuron.h:26
 
 class PopulationBase {
 public:
@@ -165,6 +214,7 @@ public:
     virtual NeuronBase *getNeuron(int idx) = 0;
     virtual Type getType() = 0;
     virtual const real *paramsOf(int idx) = 0;
+    virtual uint8_t kindOf(int idx) = 0;
     virtual real tauOf(int idx, bool inhibitory) = 0;
 };
 
@@ -174,7 +224,7 @@ public:
     Population(size_t N) : N(N) { neurons.reserve(N); }
     Population(size_t N, const Neuron &templ) : N(N), neurons(N, templ) {}
     int getNum() { return (int)N; }
-    Type getType() { return LIFE; }
+    Type getType() { return Neuron::type; }
     NeuronBase *getNeuron(int idx) { return &neurons[idx]; }
     /* Appends a neuron with its own parameters (Population.h:158-168). */
     int addNeuron(Neuron templ)
@@ -187,6 +237,7 @@ public:
         return (int)neurons.size() - 1;
     }
     const real *paramsOf(int idx) { return neurons[idx].params(); }
+    uint8_t kindOf(int idx) { (void)idx; return Neuron::kind; }
     real tauOf(int idx, bool inh) { return inh ? neurons[idx].tauSynI() : neurons[idx].tauSynE(); }
 
 private:
@@ -286,12 +337,14 @@ public:
      * order and synapses in connect() order with StaticSynapse::reset applied
      * (src/synapse/static/StaticSynapse.cpp:43-54). Returns 0 or a BSIM_ERR_* code. */
     int flatten(real dt, std::vector<float> &params, std::vector<int32_t> &pop, std::vector<int32_t> &src,
-                std::vector<int32_t> &dst, std::vector<float> &weight, std::vector<int32_t> &delay_steps)
+                std::vector<int32_t> &dst, std::vector<float> &weight, std::vector<int32_t> &delay_steps,
+                std::vector<uint8_t> *kind = NULL)
     {
         std::map<NeuronBase *, std::pair<int, int>> where;  // neuron -> (population, index)
         int g = 0;
         params.clear();
         pop.clear();
+        if (kind) kind->clear();
         for (size_t p = 0; p < pPopulations.size(); p++) {
             PopulationBase *pp = pPopulations[p];
             for (int i = 0; i < pp->getNum(); i++, g++) {
@@ -301,6 +354,7 @@ public:
                 const real *q = pp->paramsOf(i);
                 params.insert(params.end(), q, q + 10);
                 pop.push_back((int32_t)p);
+                if (kind) kind->push_back(pp->kindOf(i));
             }
         }
         totalNeuronNum = g;
@@ -379,7 +433,8 @@ public:
         const int sim_cycle = (int)round(time / dt);
         std::vector<float> params, weight;
         std::vector<int32_t> pop, src, dst, delay;
-        int rc = network->flatten(dt, params, pop, src, dst, weight, delay);
+        std::vector<uint8_t> kind;
+        int rc = network->flatten(dt, params, pop, src, dst, weight, delay, &kind);
         if (rc != BSIM_OK) return rc;
         FILE *info_file = fopen("GSim.info", "w+");
         if (!info_file) {
@@ -391,17 +446,21 @@ public:
         const char *acc = getenv("BSIM_ACCUMULATE");
         if (acc && strcmp(acc, "ordered") == 0) opt.accumulate = BSIM_ACC_ORDERED;
         const int64_t n = (int64_t)pop.size();
+        const char *seed_env = getenv("BSIM_INPUT_SEED");
+        const uint64_t seed = seed_env ? strtoull(seed_env, NULL, 10) : 1;
+        int n_types = 0;
+        for (int k = 0; k < 3; k++) n_types += std::find(kind.begin(), kind.end(), (uint8_t)k) != kind.end();
         bsim_engine *e = NULL;
-        rc = bsim_create(params.data(), n, pop.data(), NULL, src.data(), dst.data(), weight.data(), delay.data(),
-                         (int64_t)src.size(), dt, &opt, &e);
+        rc = bsim_create_mixed(params.data(), kind.data(), n, pop.data(), NULL, src.data(), dst.data(),
+                               weight.data(), delay.data(), (int64_t)src.size(), dt, seed, &opt, &e);
         if (rc != BSIM_OK) {
-            fprintf(stderr, "bsim_create: %s\n", bsim_last_error());
+            fprintf(stderr, "bsim_create_mixed: %s\n", bsim_last_error());
             fclose(info_file);
             return rc;
         }
         bsim_info inf;
         bsim_get_info(e, &inf);
-        fprintf(info_file, "NeuronTypeNum: %d, SynapseTypeNum: %d\n", 1, 1);
+        fprintf(info_file, "NeuronTypeNum: %d, SynapseTypeNum: %d\n", n_types, 1);
         fprintf(info_file, "NeuronNum: %lld, SynapseNum: %lld\n", (long long)n, (long long)src.size());
         fprintf(info_file, "MAX_DELAY: %d\n", inf.max_delay);
         fprintf(info_file, "Start runing for %d cycles\n", sim_cycle);

@@ -34,6 +34,11 @@ extern "C" {
 #define BSIM_MAX_DELAY 1024    /* delays are 1..BSIM_MAX_DELAY steps */
 #define BSIM_MAX_CLASSES 65535 /* distinct folded LIF parameter tuples per engine */
 
+/* Neuron kinds (bsim_create_mixed). */
+#define BSIM_NEURON_LIF 0      /* LIF_brian / IF_curr_exp: LIFENeuron + StaticSynapse */
+#define BSIM_NEURON_CONSTANT 1 /* Constant_spikes: ConstantNeuron + StaticSynapse */
+#define BSIM_NEURON_POISSON 2  /* Poisson_spikes: PoissonNeuron + StaticSynapse */
+
 /* How one step's synaptic input is summed per target neuron. */
 #define BSIM_ACC_EXACT 0   /* exact int64 fixed point (quantum 2^-qexp per network): the sum is
                               independent of delivery order, so push, pull, batched and
@@ -124,6 +129,29 @@ int bsim_create(const float *params, int64_t n, const int32_t *pop, const int32_
                 const int32_t *src, const int32_t *dst, const float *weight, const int32_t *delay_steps,
                 int64_t s, float dt, const bsim_options *opt, bsim_engine **out);
 
+/* bsim_create for networks that also hold input-drive neurons, Constant_spikes and
+ * Poisson_spikes (include/Neuron.h:25-26 of the reference), stepped in the same launch
+ * as the LIF neurons with the reference GPU kernels' rules:
+ *   kind[i] = BSIM_NEURON_LIF       params[i] as for bsim_create
+ *   kind[i] = BSIM_NEURON_CONSTANT  params[i][0..2] = ConstantNeuron(fire_rate, start_time,
+ *             end_time) (src/neuron/constant/ConstantNeuron.cpp:14); fires at cycle t iff
+ *             t < end_cycle and (t - start_cycle) * fire_rate > fire_count
+ *             (src/neuron/constant/constant.cu:18-22), cycles = (int)(time / dt)
+ *   kind[i] = BSIM_NEURON_POISSON   params[i][0..3] = PoissonNeuron(rate, refract, start_time,
+ *             duration) (src/neuron/poisson/PoissonNeuron.cpp:13); fires at cycle t iff
+ *             t == fire_cycle and t <= end_cycle, then fire_cycle += 1 + Poisson(rate) +
+ *             (int)(refract / dt) (src/neuron/poisson/poisson.cu:9-31); the first fire_cycle is
+ *             (int)(start_time / dt) + Poisson(rate); rate is the mean gap in cycles, 0..2^24.
+ * The reference draws Poisson numbers from a clock-seeded host generator and curand
+ * (not reproducible); here each draw is a function of (input_seed, the neuron's id minus
+ * the first id of its network, the cycle), so a run is reproducible and a network gives
+ * the same spikes alone or packed with others. Cycles beyond 2^31-1 are clamped to it.
+ * kind may be NULL (all LIF: the same engine as bsim_create). */
+int bsim_create_mixed(const float *params, const uint8_t *kind, int64_t n, const int32_t *pop,
+                      const int32_t *instance, const int32_t *src, const int32_t *dst, const float *weight,
+                      const int32_t *delay_steps, int64_t s, float dt, uint64_t input_seed,
+                      const bsim_options *opt, bsim_engine **out);
+
 /* Builds an engine for one or more generated networks directly on the device
  * (no host synapse arrays). Network k's neurons follow network k-1's. */
 int bsim_create_generated(const bsim_gen_spec *specs, int32_t n_specs, float dt, const bsim_options *opt,
@@ -162,7 +190,10 @@ int bsim_record(bsim_engine *e, int64_t max_steps, int64_t capacity);
 int bsim_read_raster(bsim_engine *e, int64_t *step_off, int32_t *ids, int64_t ids_cap, int64_t *n_steps);
 
 /* Neuron state: v, i_E, i_I, refrac_step per neuron (cudaFetchLIFE,
- * src/neuron/lif/GLIFENeurons.cu:29-40). Any pointer may be NULL. */
+ * src/neuron/lif/GLIFENeurons.cu:29-40). Any pointer may be NULL. For input-drive
+ * neurons the four slots hold, as float / float bits / float bits / int:
+ * Constant {fire_rate, start_cycle, end_cycle, fire_count}, Poisson {rate, fire_cycle,
+ * end_cycle, refrac_step} (ints in the middle two slots as their bit patterns). */
 int bsim_read_state(bsim_engine *e, float *v, float *i_E, float *i_I, int32_t *refrac_step);
 
 /* Overwrites the neuron state from host arrays (the state half of copyNetworkToGPU,
@@ -238,9 +269,11 @@ typedef struct bsim_pred_stats {
 int bsim_predictor_stats(bsim_engine *e, bsim_pred_stats *stats);
 
 /* Autotuner (replaces the occupancy rule of getBlockSize, src/gpu_utils/gpu_func.cu:90-127):
- * runs trial_steps cycles for each candidate (block size, grid, delivery mode),
- * keeps the fastest and reports each mode's measured cost. The simulation advances
- * by the trial cycles (the dynamics are the same for every candidate). */
+ * runs trial_steps cycles for each candidate (block size, grid, delivery mode) in
+ * three interleaved rounds (so that every candidate sees the same drift of the
+ * network's activity), keeps the one with the least summed time and reports each
+ * mode's measured cost. The simulation advances by 3 x candidates x trial_steps
+ * cycles (the dynamics are the same for every candidate). */
 typedef struct bsim_tune_result {
     int32_t block_threads, grid_blocks, delivery;
     float best_us_per_step;
@@ -303,6 +336,9 @@ typedef struct bsim_class_params {
     int32_t refrac_time;
     float scale_up, scale_down;
     int32_t pop, inst;
+    int32_t kind;        /* BSIM_NEURON_LIF (the only kind this entry point takes) */
+    int32_t id_base;     /* 0 */
+    int32_t reserved[2]; /* 0 */
 } bsim_class_params;
 
 int bsim_run_noalloc(int64_t n, int32_t max_delay, void *state_dev, const float *vtmp_dev, const uint16_t *cls_dev,

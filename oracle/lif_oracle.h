@@ -15,6 +15,14 @@
  *                       -> NeuronBase::fire        src/base/NeuronBase.cpp:47-54
  *                       -> StaticSynapse::recv/update src/synapse/static/StaticSynapse.cpp:31-70
  *                       -> LIFENeuron::recv        src/neuron/lif/LIFENeuron.cpp:52-61
+ *   input-drive neurons (kind 1, 2) follow the reference's GPU kernels, whose rules
+ *   differ from its CPU classes (the engine replaces SGSim):
+ *                       ConstantNeuron  src/neuron/constant/constant.cu:18-22,
+ *                                       reset ConstantNeuron.cpp:55-62
+ *                       PoissonNeuron   src/neuron/poisson/poisson.cu:9-31,
+ *                                       reset PoissonNeuron.cpp:35-44
+ *   with the engine's reproducible Poisson sampler restated in lif_oracle.c (the
+ *   reference's draws come from clock-seeded generators and cannot be replayed).
  *
  * Parity is pinned in tests against the reference's golden traces
  * (test/lif_unit{1..4}_test_v.std) and against the reference sources compiled
@@ -56,7 +64,18 @@ typedef struct oracle_out {
      * (t / half_period) is odd. params_alt may differ from params in i_offset only. */
     const void *params_alt;
     int64_t half_period;  /* 0: constant drive */
+    /* Optional input-drive neurons (inputs as well). kind[j]: 0 LIF_brian, 1 Constant_spikes,
+     * 2 Poisson_spikes (NULL = all LIF); params[j] then holds ConstantNeuron(fire_rate,
+     * start_time, end_time) or PoissonNeuron(rate, refract, start_time, duration) in its
+     * first slots. instance[j] (NULL = one network) and input_seed key the Poisson draws. */
+    const uint8_t *kind;
+    const int32_t *instance;
+    uint64_t input_seed;
 } oracle_out;
+
+/* The Poisson sampler on its own: n draws of Poisson(rate), draw i keyed as the
+ * initial draw of neuron id i (statistics checks). */
+int oracle_poisson_draws(uint64_t seed, float rate, int64_t n, int32_t *out);
 
 /* ---- float build (reference `real` = float) ---- */
 int oracle_lif_reset_f32(const float *params, int64_t n, float dt, float *fold, int32_t *refrac_time);

@@ -113,12 +113,62 @@ int SFX(oracle_run)(const REAL *params, int64_t n,
     int64_t ev_cap = 1024;
     int64_t *ev = (int64_t *)malloc(sizeof(int64_t) * (size_t)ev_cap);
     REAL *vtmp_base = NULL, *vtmp_alt = NULL; /* square-wave drive: v_tmp of each phase */
+    /* input-drive neurons: Constant {start_cycle, end_cycle, fire_count},
+     * Poisson {fire_cycle, end_cycle, refrac_step}, and each neuron's draw id */
+    int32_t *dslot = NULL;
+    int64_t *draw_id = NULL;
+    const uint8_t *kind = out->kind;
     int rc = 0;
     if (!fold || !rtime || !rstep || !synE || !synI || !accE || !accI || !off || !ids || !ring || !ring_n || !ev) {
         rc = -4;
         goto done;
     }
     SFX(oracle_lif_reset)(params, n, dt, fold, rtime);
+    if (kind) {
+        dslot = (int32_t *)calloc((size_t)n * 3, sizeof(int32_t));
+        draw_id = (int64_t *)malloc(sizeof(int64_t) * (size_t)n);
+        if (!dslot || !draw_id || o_tables()) { rc = -4; goto done; }
+        /* Poisson draws are keyed by (seed, id - first id of the neuron's network, cycle) */
+        if (out->instance) {
+            int32_t ninst = 1;
+            for (int64_t j = 0; j < n; j++) {
+                if (out->instance[j] < 0) { rc = -1; goto done; }
+                if (out->instance[j] >= ninst) ninst = out->instance[j] + 1;
+            }
+            int64_t *first = (int64_t *)malloc(sizeof(int64_t) * (size_t)ninst);
+            if (!first) { rc = -4; goto done; }
+            for (int32_t g = 0; g < ninst; g++) first[g] = -1;
+            for (int64_t j = 0; j < n; j++) {
+                if (first[out->instance[j]] < 0) first[out->instance[j]] = j;
+                draw_id[j] = j - first[out->instance[j]];
+            }
+            free(first);
+        } else {
+            for (int64_t j = 0; j < n; j++) draw_id[j] = j;
+        }
+        for (int64_t j = 0; j < n; j++) {
+            const REAL *p = params + j * ORACLE_NPARAM;
+            int32_t *ds = dslot + 3 * j;
+            if (kind[j] == 1) {
+                /* ConstantNeuron::reset (src/neuron/constant/ConstantNeuron.cpp:55-62) */
+                ds[0] = R_CYCLE(p[1] / dt);
+                ds[1] = R_CYCLE(p[2] / dt);
+                ds[2] = 0;
+            } else if (kind[j] == 2) {
+                /* PoissonNeuron::reset (src/neuron/poisson/PoissonNeuron.cpp:35-44) */
+                float rate = (float)p[0];
+                if (!(rate >= 0.0f && rate < 16777216.0f)) { rc = -1; goto done; }
+                int64_t fc = (int64_t)R_CYCLE(p[2] / dt) +
+                             o_poisson_draw(o_poisson_key(out->input_seed, draw_id[j], -1), rate);
+                ds[0] = fc > INT32_MAX ? INT32_MAX : (int32_t)fc;
+                ds[1] = R_CYCLE((p[2] + p[3]) / dt);
+                ds[2] = R_CYCLE(p[1] / dt);
+            } else if (kind[j] != 0) {
+                rc = -1;
+                goto done;
+            }
+        }
+    }
     if (out->params_alt && out->half_period > 0) {
         REAL *fa = (REAL *)malloc(sizeof(REAL) * ORACLE_NFOLD * (size_t)n);
         int32_t *ra = (int32_t *)malloc(sizeof(int32_t) * (size_t)n);
@@ -175,7 +225,25 @@ int SFX(oracle_run)(const REAL *params, int64_t n,
                 in_I = synI[j];
             }
             int fired = 0;
-            if (rstep[j] > 0) {
+            if (kind && kind[j] == 1) {
+                /* update_constant_neuron (src/neuron/constant/constant.cu:18-22) */
+                int32_t *ds = dslot + 3 * j;
+                REAL rate = params[j * ORACLE_NPARAM];
+                if ((int32_t)t < ds[1] && (REAL)((int32_t)t - ds[0]) * rate > (REAL)ds[2]) {
+                    fired = 1;
+                    ds[2]++;
+                }
+            } else if (kind && kind[j] == 2) {
+                /* update_poisson_neuron + reset_poisson_neuron (src/neuron/poisson/poisson.cu:29-31, 9-15) */
+                int32_t *ds = dslot + 3 * j;
+                if ((int32_t)t == ds[0] && (int32_t)t <= ds[1]) {
+                    fired = 1;
+                    float rate = (float)params[j * ORACLE_NPARAM];
+                    int64_t nxt = (int64_t)ds[0] + 1 +
+                                  o_poisson_draw(o_poisson_key(out->input_seed, draw_id[j], ds[0]), rate) + ds[2];
+                    ds[0] = nxt > INT32_MAX ? INT32_MAX : (int32_t)nxt;
+                }
+            } else if (rstep[j] > 0) {
                 --rstep[j];
             } else {
                 REAL vm = f[10] * f[0] + f[5] + f[7] * f[4] + f[6] * f[3];
@@ -255,6 +323,14 @@ int SFX(oracle_run)(const REAL *params, int64_t n,
     if (out->final_state) {
         REAL *fs = (REAL *)out->final_state;
         for (int64_t j = 0; j < n; j++) {
+            if (kind && kind[j] != 0) {
+                /* drive neurons: rate, then their three counters */
+                fs[j * 4 + 0] = params[j * ORACLE_NPARAM];
+                fs[j * 4 + 1] = (REAL)dslot[3 * j];
+                fs[j * 4 + 2] = (REAL)dslot[3 * j + 1];
+                fs[j * 4 + 3] = (REAL)dslot[3 * j + 2];
+                continue;
+            }
             fs[j * 4 + 0] = fold[j * ORACLE_NFOLD + 0];
             fs[j * 4 + 1] = fold[j * ORACLE_NFOLD + 7];
             fs[j * 4 + 2] = fold[j * ORACLE_NFOLD + 6];
@@ -262,6 +338,7 @@ int SFX(oracle_run)(const REAL *params, int64_t n,
         }
     }
 done:
+    free(dslot); free(draw_id);
     free(vtmp_base); free(vtmp_alt);
     free(fold); free(rtime); free(rstep); free(synE); free(synI); free(accE); free(accI);
     free(off); free(ids); free(ring); free(ring_n); free(ev);

@@ -53,6 +53,8 @@ def lib():
             f = getattr(L, "oracle_run_" + sfx)
             f.argtypes = [P, i64, P, P, P, P, i64, real, i64, ctypes.c_int, P, P]
             f.restype = ctypes.c_int
+        L.oracle_poisson_draws.argtypes = [ctypes.c_uint64, ctypes.c_float, i64, P]
+        L.oracle_poisson_draws.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -72,6 +74,9 @@ class _Out(ctypes.Structure):
         ("events_per_step", ctypes.c_void_p),
         ("params_alt", ctypes.c_void_p),
         ("half_period", ctypes.c_int64),
+        ("kind", ctypes.c_void_p),
+        ("instance", ctypes.c_void_p),
+        ("input_seed", ctypes.c_uint64),
     ]
 
 
@@ -106,10 +111,12 @@ def syn_reset(delay_s, weight, tau_syn, dt, dtype=np.float32):
 
 
 def run(params, src, dst, weight, delay_steps, dt, steps, record_steps=0, rec_ids=None,
-        acc_mode=ACC_SEQUENTIAL, qexp=None, dtype=np.float32, raster_cap=None, params_alt=None, half_period=0):
+        acc_mode=ACC_SEQUENTIAL, qexp=None, dtype=np.float32, raster_cap=None, params_alt=None, half_period=0,
+        kind=None, instance=None, input_seed=0):
     """Run the oracle. Returns a dict with fire_count, raster (list of arrays),
     v_trace [record_steps, n_rec], final_state [n, 4], spikes/events per step.
-    params_alt / half_period: square-wave drive (params_alt's v_tmp in odd half periods)."""
+    params_alt / half_period: square-wave drive (params_alt's v_tmp in odd half periods).
+    kind / instance / input_seed: input-drive neurons (0 LIF, 1 Constant, 2 Poisson)."""
     params = np.ascontiguousarray(params, dtype=dtype)
     n = params.shape[0]
     src = np.ascontiguousarray(src, dtype=np.int32)
@@ -134,9 +141,13 @@ def run(params, src, dst, weight, delay_steps, dt, steps, record_steps=0, rec_id
         qexp = np.ascontiguousarray(np.broadcast_to(np.asarray(qexp, dtype=np.int32), (n,)))
     if params_alt is not None:
         params_alt = np.ascontiguousarray(params_alt, dtype=dtype)
+    if kind is not None:
+        kind = np.ascontiguousarray(kind, dtype=np.uint8)
+    if instance is not None:
+        instance = np.ascontiguousarray(instance, dtype=np.int32)
     out = _Out(record_steps, _ptr(fire_count), _ptr(raster_off), _ptr(raster_ids), raster_cap,
                _ptr(rec_ids), rec_ids.shape[0], _ptr(v_trace), _ptr(final_state), _ptr(spikes),
-               _ptr(events), _ptr(params_alt), int(half_period))
+               _ptr(events), _ptr(params_alt), int(half_period), _ptr(kind), _ptr(instance), int(input_seed))
     sfx = "f32" if dtype == np.float32 else "f64"
     rc = getattr(lib(), "oracle_run_" + sfx)(
         _ptr(params), n, _ptr(src), _ptr(dst), _ptr(weight), _ptr(delay_steps), s, dt, steps,
@@ -146,6 +157,15 @@ def run(params, src, dst, weight, delay_steps, dt, steps, record_steps=0, rec_id
     raster = [raster_ids[raster_off[t]:raster_off[t + 1]].copy() for t in range(record_steps)]
     return dict(fire_count=fire_count, raster=raster, v_trace=v_trace, final_state=final_state,
                 spikes_per_step=spikes, events_per_step=events)
+
+
+def poisson_draws(seed, rate, n):
+    """n draws of the engine's Poisson sampler (draw i keyed as neuron i's first draw)."""
+    out = np.zeros(n, dtype=np.int32)
+    rc = lib().oracle_poisson_draws(int(seed), float(rate), int(n), _ptr(out))
+    if rc != 0:
+        raise RuntimeError("oracle_poisson_draws failed with code %d" % rc)
+    return out
 
 
 def ref_available(precision="f32"):

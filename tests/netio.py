@@ -74,3 +74,53 @@ def syn_tau(net):
     pop_of = np.repeat(np.arange(len(net["pop_size"])), net["pop_size"])
     tp = pop_of[net["dst"]]
     return np.where(net["type"] == 0, net["pop_tau"][tp, 0], net["pop_tau"][tp, 1])
+
+
+def drive_net(seed=1, lif_size=200):
+    """A network with input-drive neurons (kind 2 Poisson_spikes, kind 1 Constant_spikes)
+    feeding two LIF_brian populations, in float32 engine form (dt = 0.1 ms).
+
+    Population 0: 70 Poisson neurons, rates 3.5 .. 20000.5 cycles (every level of the
+      sampler), refract 0 / 0.5 ms, start 0 / 10 ms, durations 1000 s or 0.2 s.
+    Population 1: 20 Constant neurons, fire_rate 0.4 / 0.05 / 1.0 / 0.013 per cycle,
+      start 5 ms, end 150 ms or 1e9 s (clamped).
+    Populations 2, 3: LIF_brian, subthreshold i_offset; 0 -> 2, 1 -> 3, 2 -> 3 (E),
+      3 -> 2 (I), and 2 -> 0 (input that drive neurons ignore). Delays U{1..8} steps.
+    Returns params [n, 10], kind [n], pop [n], src, dst, weight, delay_steps."""
+    rng = np.random.default_rng(seed)
+    rates = np.repeat([3.5, 20.0, 70.25, 300.0, 1500.0, 6000.0, 20000.5], 10).astype(np.float32)
+    nP, nC, nL = rates.size, 20, lif_size
+    n = nP + nC + 2 * nL
+    params = np.zeros((n, 10), np.float32)
+    kind = np.zeros(n, np.uint8)
+    pop = np.repeat(np.arange(4, dtype=np.int32), [nP, nC, nL, nL])
+    i = np.arange(nP)
+    kind[:nP] = 2
+    params[:nP, 0] = rates
+    params[:nP, 1] = np.where(i % 2 == 0, 0.0, 5e-4)
+    params[:nP, 2] = np.where((i // 2) % 2 == 0, 0.0, 1e-2)
+    params[:nP, 3] = np.where(i % 5 == 4, 0.2, 1000.0)
+    c = np.arange(nC)
+    kind[nP:nP + nC] = 1
+    params[nP:nP + nC, 0] = np.array([0.4, 0.05, 1.0, 0.013], np.float32)[c % 4]
+    params[nP:nP + nC, 1] = 5e-3
+    params[nP:nP + nC, 2] = np.where(c < nC // 2, 0.15, 1e9)
+    lif = [-0.065, -0.065, -0.065, 0.25e-9, 20e-3, 2e-3, 5e-3, 10e-3, -0.050, 0.0]
+    params[nP + nC:] = lif
+    params[nP + nC:, 0] = rng.uniform(-0.065, -0.055, 2 * nL)
+    params[nP + nC:, 9] = rng.uniform(0.0, 0.15e-9, 2 * nL)
+    base = [0, nP, nP + nC, nP + nC + nL]
+    size = [nP, nC, nL, nL]
+    src, dst, w = [], [], []
+    for a, b, p, lo, hi in [(0, 2, 0.2, 0.0, 2e-9), (1, 3, 0.5, 0.0, 3e-10), (2, 3, 0.1, 0.0, 2e-10),
+                            (3, 2, 0.1, -4e-10, 0.0), (2, 0, 0.05, 0.0, 1e-10)]:
+        m = rng.random((size[a], size[b])) < p
+        s_, d_ = np.nonzero(m)
+        src.append(s_ + base[a])
+        dst.append(d_ + base[b])
+        w.append(rng.uniform(lo, hi, s_.size))
+    src = np.concatenate(src).astype(np.int32)
+    dst = np.concatenate(dst).astype(np.int32)
+    weight = np.concatenate(w).astype(np.float32)
+    delay = rng.integers(1, 9, src.size).astype(np.int32)
+    return dict(params=params, kind=kind, pop=pop, src=src, dst=dst, weight=weight, delay_steps=delay)

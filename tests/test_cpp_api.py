@@ -17,8 +17,8 @@ SRC = os.path.join(ROOT, "tests", "cpp", "lif_api_demo.cpp")
 GOLDEN = np.load(os.path.join(ROOT, "tests", "golden", "lif_unit_v.npz"))
 
 
-def compile_demo(out, log_data):
-    cmd = ["g++", "-std=c++11", "-O2", "-Wall", "-Werror", "-I" + os.path.join(ROOT, "include"), SRC,
+def compile_demo(out, log_data, src=SRC):
+    cmd = ["g++", "-std=c++11", "-O2", "-Wall", "-Werror", "-I" + os.path.join(ROOT, "include"), src,
            "-L" + os.path.dirname(B.LIB_PATH), "-lbsim_b200", "-Wl,-rpath," + os.path.dirname(B.LIB_PATH), "-o", out]
     if log_data:
         cmd.insert(1, "-DLOG_DATA")
@@ -73,3 +73,51 @@ def test_sgsim_plain_build_writes_fire_count(demos):
         subprocess.run([demos[0], "2"], cwd=d, check=True, stdout=subprocess.DEVNULL)
         count = np.loadtxt(os.path.join(d, "GFire.count"), dtype=np.int64)
     assert np.array_equal(count, ref["fire_count"])
+
+
+DRIVE_SRC = os.path.join(ROOT, "tests", "cpp", "drive_api_demo.cpp")
+
+
+@pytest.fixture(scope="module")
+def drive_demo(tmp_path_factory):
+    out = str(tmp_path_factory.mktemp("cppdrive") / "drive_demo")
+    compile_demo(out, False, DRIVE_SRC)
+    return out
+
+
+def test_drive_program_compiles(drive_demo):
+    assert os.path.exists(drive_demo)
+
+
+def drive_demo_oracle(seed):
+    """The network of tests/cpp/drive_api_demo.cpp in flat form, run by the oracle."""
+    NC, NP, NL = 4, 6, 8
+    params = np.zeros((NC + NP + NL, 10), np.float32)
+    params[:NC, :3] = [0.02, 0.0, 0.15]
+    params[NC:NC + NP, :4] = [40.0, 1e-3, 0.005, 1000.0]
+    params[NC + NP:] = [-0.065, -0.065, -0.065, 0.25e-9, 20e-3, 2e-3, 5e-3, 10e-3, -0.050, 0.1e-9]
+    kind = np.array([1] * NC + [2] * NP + [0] * NL, np.uint8)
+    i_c, i_p = np.arange(NC * NL), np.arange(NP * NL)
+    src = np.concatenate([i_c // NL, NC + i_p // NL]).astype(np.int32)
+    dst = np.concatenate([NC + NP + i_c % NL, NC + NP + i_p % NL]).astype(np.int32)
+    wc = np.float32(1e-9) + np.float32(1e-10) * (i_c % 7).astype(np.float32)
+    wp = np.float32(2e-9) - np.float32(1e-10) * (i_p % 5).astype(np.float32)
+    delay = np.concatenate([np.full(NC * NL, 2e-4), np.full(NP * NL, 5e-4)]).astype(np.float32)
+    tau = np.concatenate([np.full(NC * NL, 1e-3), np.full(NP * NL, 1e-3)]).astype(np.float32)
+    st, w = oracle.syn_reset(delay, np.concatenate([wc, wp]), tau, np.float32(1e-4))
+    return oracle.run(params, src, dst, w, st, np.float32(1e-4), 2000, kind=kind, input_seed=seed)
+
+
+@pytest.mark.gpu
+def test_drive_program_fire_count_matches_oracle(drive_demo):
+    """GFire.count of the program equals the oracle's spike counts (Poisson draws
+    seeded by BSIM_INPUT_SEED); the LIF population is driven into firing."""
+    with tempfile.TemporaryDirectory() as d:
+        env = dict(os.environ, BSIM_INPUT_SEED="3")
+        subprocess.run([drive_demo], cwd=d, check=True, env=env, stdout=subprocess.DEVNULL)
+        count = np.loadtxt(os.path.join(d, "GFire.count"), dtype=np.int64)
+        info = open(os.path.join(d, "GSim.info")).read()
+    ref = drive_demo_oracle(3)
+    assert "NeuronTypeNum: 3" in info
+    assert np.array_equal(count, ref["fire_count"])
+    assert ref["fire_count"][10:].sum() > 0

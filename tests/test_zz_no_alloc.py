@@ -20,7 +20,8 @@ DT = np.float32(1e-4)
 
 CLASS_DTYPE = np.dtype([("Cm", "<f4"), ("CE", "<f4"), ("CI", "<f4"), ("C_E", "<f4"), ("C_I", "<f4"),
                         ("v_thresh", "<f4"), ("v_reset", "<f4"), ("refrac_time", "<i4"), ("scale_up", "<f4"),
-                        ("scale_down", "<f4"), ("pop", "<i4"), ("inst", "<i4")])
+                        ("scale_down", "<f4"), ("pop", "<i4"), ("inst", "<i4"), ("kind", "<i4"),
+                        ("id_base", "<i4"), ("reserved", "<i4", (2,))])
 
 
 def noalloc_fn():
@@ -43,7 +44,7 @@ def caller_buffers(g, qexp, D):
     for p in range(P):
         i = int(np.flatnonzero(pops == p)[0])
         ctab[p] = (fold[i, 10], fold[i, 2], fold[i, 1], fold[i, 4], fold[i, 3], fold[i, 8], fold[i, 9], rt[i],
-                   np.ldexp(np.float32(1), qexp), np.ldexp(np.float32(1), -qexp), p, 0)
+                   np.ldexp(np.float32(1), qexp), np.ldexp(np.float32(1), -qexp), p, 0, 0, 0, (0, 0))
     state = np.zeros((n, 4), np.float32)
     state[:, 0] = params[:, 0]
     key = g["src"].astype(np.int64) * D + (g["delay_steps"] - 1)
