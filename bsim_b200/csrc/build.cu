@@ -429,6 +429,10 @@ static int create_from_arrays(const float *params, const uint8_t *kind, int64_t 
     return BSIM_OK;
 }
 
+#ifndef MAX_PLANES
+#define MAX_PLANES 8  // parts per tile (accumulator planes)
+#endif
+
 // Ring, bitmaps, accumulators, counters; launch shape. Shared by both builders.
 static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
 {
@@ -442,10 +446,39 @@ static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
     TRY(dalloc(e, &d_ctab, ctab.size()));
     CK(cudaMemcpy(d_ctab, ctab.data(), sizeof(ClassParams) * ctab.size(), cudaMemcpyHostToDevice));
     a.ctab = d_ctab;
-    size_t acc_elem = e.opt.accumulate == BSIM_ACC_ORDERED ? sizeof(float2) : sizeof(longlong2);
+    // tiled delivery: each tile's work units in n_planes parts, one accumulator
+    // plane per part; about two parts per resident block (occupancy 2 blocks/SM)
+    a.n_planes = 1;
+    a.n_parts = 0;
+    a.parts = nullptr;
+    if (a.n_tiles > 0) {
+        const int nt = a.n_tiles;
+        const double want = 4.0 * e.sm_count / nt;
+        a.n_planes = (int32_t)std::max(1.0, std::min((double)MAX_PLANES, std::floor(want + 0.5)));
+        const int P = a.n_planes;
+        std::vector<int4> parts;
+        for (int q = 0; q < nt; q++) {
+            const int U = q < (int)e.tile_units.size() ? e.tile_units[q] : 0;
+            for (int k = 0; k < P; k++)
+                parts.push_back(make_int4(q, (int)((int64_t)U * k / P), (int)((int64_t)U * (k + 1) / P), k));
+        }
+        // largest expected work first, so the queue ends with small parts
+        std::stable_sort(parts.begin(), parts.end(), [&](const int4 &x, const int4 &y) {
+            const int64_t ex = x.x < (int)e.tile_entries.size() ? e.tile_entries[x.x] : 0;
+            const int64_t ey = y.x < (int)e.tile_entries.size() ? e.tile_entries[y.x] : 0;
+            return ex > ey;
+        });
+        int4 *d_parts;
+        TRY(dalloc(e, &d_parts, parts.size()));
+        CK(cudaMemcpy(d_parts, parts.data(), sizeof(int4) * parts.size(), cudaMemcpyHostToDevice));
+        a.parts = d_parts;
+        a.n_parts = (int32_t)parts.size();
+    }
+    const size_t acc_elem = e.opt.accumulate == BSIM_ACC_ORDERED ? sizeof(float2) : sizeof(longlong2);
+    const size_t acc_count = 2 * (size_t)a.n_planes * (size_t)e.N;
     char *d_acc;
-    TRY(dalloc(e, &d_acc, acc_elem * 2 * (size_t)e.N));
-    CK(cudaMemset(d_acc, 0, acc_elem * 2 * (size_t)e.N));
+    TRY(dalloc(e, &d_acc, acc_elem * acc_count));
+    CK(cudaMemset(d_acc, 0, acc_elem * acc_count));
     a.acc = d_acc;
     uint32_t *d_bm;
     TRY(dalloc(e, &d_bm, (size_t)a.R * a.W));
@@ -469,6 +502,7 @@ static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
     a.step_ctr = d_ctr;
     a.events = d_ctr + 1;
     a.ticket = reinterpret_cast<unsigned int *>(d_ctr + 2);
+    a.part_ctr = reinterpret_cast<unsigned int *>(d_ctr + 3);
     a.delivery = (e.opt.delivery == BSIM_DELIVERY_PULL || e.opt.delivery == BSIM_DELIVERY_AUTO) ? e.opt.delivery
                                                                                                  : BSIM_DELIVERY_PUSH;
     a.deliv_sel = nullptr;
@@ -479,6 +513,9 @@ static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
     a.n_pops = e.n_pops;
     a.hist_len = 0;
     if (a.n_tiles > 0 && e.opt.delivery == BSIM_DELIVERY_TILE) a.delivery = BSIM_DELIVERY_TILE;
+    // every cycle of a tiled-only engine overwrites all planes of the parity it
+    // delivers into, so the LIF phase need not clear them; any other mode adds
+    a.acc_clear = a.delivery == BSIM_DELIVERY_TILE ? 0 : 1;
     // launch shape: all blocks resident (occupancy-sized grid), so the grid-stride
     // loops of both phases see every SM
     e.block = e.opt.block_threads > 0 ? e.opt.block_threads : 512;
@@ -514,14 +551,18 @@ static int plan_tiles(const std::vector<int64_t> &run_beg, int64_t tile, std::ve
     return BSIM_OK;
 }
 
-// 16 bytes of shared counters per target (four u32 limbs, one sign): tiles of
-// <= 6144 targets let two 512-thread blocks share an SM; large populations are
-// split into equal tiles, small networks into enough tiles to fill the GPU.
-static int64_t auto_tile_size(const bsim_options &o, int64_t N, int sm_count)
+// 16 bytes of shared counters per target (two words per E and I sum): tiles of
+// <= 5000 targets let two 512-thread blocks share an SM. Every tile scans the
+// fire bitmaps of its sources for each delay, so that cost grows with tiles x D,
+// while more tiles balance the blocks better. Measured on the generator's
+// networks (D = 6: 400 tiles of 2,500 beat 200 of 5,000; D = 50: 200 beat 400):
+// about 2.7 tiles per SM for short delays, 1.35 for long ones.
+static int64_t auto_tile_size(const bsim_options &o, int64_t N, int sm_count, int32_t D)
 {
     if (o.tile_size > 0) return std::min<int64_t>(o.tile_size, 12288);
-    int64_t t = (N + sm_count - 1) / sm_count;
-    return std::max<int64_t>(256, std::min<int64_t>(6144, t));
+    const double per_sm = D <= 8 ? 2.7 : 1.35;
+    const int64_t t = (int64_t)std::ceil((double)N / (per_sm * sm_count));
+    return std::max<int64_t>(256, std::min<int64_t>(5000, t));
 }
 
 static bool wants_tiles(const bsim_options &o, int32_t D)
@@ -532,7 +573,7 @@ static bool wants_tiles(const bsim_options &o, int32_t D)
 
 // Host-side description of the tiled copy.
 struct TileHost {
-    int32_t n_u = 0;  // target ranges; signed tile q covers range q % n_u with sign q / n_u
+    int32_t n_u = 0;  // tiles (target ranges)
     std::vector<int32_t> tile_beg, tile_run_off, tile_units, run_n, run_unit0;
     std::vector<float> tile_scale;
     std::vector<uint32_t> run_src0;
@@ -583,6 +624,7 @@ static int upload_tiles(Engine &e, const TileHost &th)
     }
     a.n_tiles = nt;
     a.n_tiles_u = th.n_u;
+    e.tile_units = th.tile_units;
     a.tile_max = th.tile_max;
     a.tile_beg = d_tb;
     a.tile_scale = d_ts;
@@ -596,51 +638,58 @@ static int upload_tiles(Engine &e, const TileHost &th)
 }
 
 // Host construction of the tiled copy: target ranges follow population (and
-// network) boundaries; synapses sorted by (sign, range of the target, source,
-// delay); one pair per distinct (signed tile, source), runs of consecutive
-// sources. Excitatory tiles come first (they carry most of the synapses).
+// network) boundaries; synapses sorted by (tile of the target, source, delay);
+// one pair per distinct (tile, source), runs of consecutive sources.
 static int build_tiles_host(Engine &e, const int32_t *inst, const int32_t *pop, const int32_t *src,
                             const int32_t *dst, const float *weight, const int32_t *delay, int64_t s)
 {
     const int64_t n = e.N;
     const int32_t D = e.D;
-    std::vector<int64_t> indeg(n, 0);
-    for (int64_t k = 0; k < s; k++)
-        if (++indeg[dst[k]] > 65535) return fail(BSIM_ERR_LIMIT, "tiled delivery: a neuron has more than 65535 synapses in");
     std::vector<int64_t> runs = {0};
     for (int64_t i = 1; i < n; i++)
         if ((inst && inst[i] != inst[i - 1]) || (pop && pop[i] != pop[i - 1])) runs.push_back(i);
     runs.push_back(n);
     TileHost th;
-    plan_tiles(runs, auto_tile_size(e.opt, n, e.sm_count), th.tile_beg, th.tile_max);
+    plan_tiles(runs, auto_tile_size(e.opt, n, e.sm_count, D), th.tile_beg, th.tile_max);
     th.n_u = (int32_t)th.tile_beg.size() - 1;
-    const int32_t nu = th.n_u, nt = 2 * nu;
+    const int32_t nu = th.n_u, nt = nu;
     std::vector<int32_t> tile_of(n);
     for (int32_t q = 0; q < nu; q++)
         for (int64_t i = th.tile_beg[q]; i < th.tile_beg[q + 1]; i++) tile_of[i] = q;
-    // signed tile (<= 2^27) | source (< 2^31) | delay - 1 (< 64)
+    // tile (< 2^27) | source (< 2^31) | delay - 1 (< 64)
     std::vector<std::pair<uint64_t, int64_t>> key(s);
     for (int64_t k = 0; k < s; k++) {
-        const uint64_t q = (uint64_t)(weight[k] >= 0.0f ? 0 : nu) + (uint64_t)tile_of[dst[k]];
+        const uint64_t q = (uint64_t)tile_of[dst[k]];
         key[k] = {(q << 37) | ((uint64_t)src[k] << 6) | (uint64_t)(delay[k] - 1), k};
     }
     std::sort(key.begin(), key.end());
     th.tile_scale.resize(nt);
-    for (int32_t q = 0; q < nt; q++) th.tile_scale[q] = ldexpf(1.0f, e.qexp[inst ? inst[th.tile_beg[q % nu]] : 0]);
+    for (int32_t q = 0; q < nt; q++) th.tile_scale[q] = ldexpf(1.0f, e.qexp[inst ? inst[th.tile_beg[q]] : 0]);
     th.tile_run_off.assign(nt + 1, 0);
     std::vector<int64_t> pair_base;
     std::vector<uint16_t> pair_doff;
-    std::vector<uint16_t> ent_tgt(s);
-    std::vector<float> ent_w(s);
+    std::vector<uint2> ent;
+    ent.reserve((size_t)s + (size_t)s / 8 + 16);
+    const uint2 pad = make_uint2(TILE_PAD, TILE_PAD);
     std::vector<int64_t> cnt(D);
+    int32_t cur_d = -1;
+    auto close_group = [&]() {  // pads the current (pair, delay) segment to even length
+        if (cur_d >= 0 && (cnt[cur_d] & 1)) {
+            ent.push_back(pad);
+            cnt[cur_d]++;
+        }
+        cur_d = -1;
+    };
     int32_t cur_tile = -1;
     int64_t cur_src = -1, run_start_src = -1, run_pair0 = 0;
+    bool pair_overflow = false;
     auto close_pair = [&]() {
         int64_t c = 0;
         for (int d = 0; d <= D; d++) {
             pair_doff.push_back((uint16_t)c);
             if (d < D) c += cnt[d];
         }
+        pair_overflow |= c > 65535;
         std::fill(cnt.begin(), cnt.end(), 0);
     };
     auto close_run = [&]() {
@@ -656,6 +705,7 @@ static int build_tiles_host(Engine &e, const int32_t *inst, const int32_t *pop, 
     for (int64_t pos = 0; pos < s; pos++) {
         const int64_t k = key[pos].second;
         const int32_t q = (int32_t)(key[pos].first >> 37);
+        if (q != cur_tile || src[k] != cur_src || delay[k] - 1 != cur_d) close_group();
         if (q != cur_tile || src[k] != cur_src) {
             if (cur_src >= 0) close_pair();
             const bool extends = q == cur_tile && src[k] == cur_src + 1;
@@ -667,36 +717,38 @@ static int build_tiles_host(Engine &e, const int32_t *inst, const int32_t *pop, 
             }
             cur_tile = q;
             cur_src = src[k];
-            pair_base.push_back(pos);
+            pair_base.push_back((int64_t)ent.size());
         }
-        cnt[delay[k] - 1]++;
-        ent_tgt[pos] = (uint16_t)(dst[k] - th.tile_beg[q % nu]);
-        ent_w[pos] = weight[k];
+        cur_d = delay[k] - 1;
+        cnt[cur_d]++;
+        ent.push_back(make_uint2((uint32_t)(dst[k] - th.tile_beg[q]), f2u(weight[k])));
     }
+    close_group();
     if (cur_src >= 0) {
         close_pair();
         close_run();
     }
+    e.tile_entries.assign(nt, 0);
+    for (int32_t q = 0; q < nt; q++)
+        for (int32_t r = th.tile_run_off[q]; r < th.tile_run_off[q + 1]; r++)
+            for (int32_t i = 0; i < th.run_n[r]; i++)
+                e.tile_entries[q] += pair_doff[(size_t)(th.run_pair0[r] + i) * (D + 1) + D];
     open_tiles_until(nt - 1);
+    if (pair_overflow) return fail(BSIM_ERR_LIMIT, "tiled delivery: a source has more than 65535 synapses into one tile");
     int64_t *d_pb;
-    uint16_t *d_pd, *d_et;
-    float *d_ew;
+    uint16_t *d_pd;
+    uint2 *d_ent;
     TRY(dalloc(e, &d_pb, pair_base.size()));
     TRY(dalloc(e, &d_pd, pair_doff.size()));
-    TRY(dalloc(e, &d_et, s));
-    TRY(dalloc(e, &d_ew, s));
+    TRY(dalloc(e, &d_ent, ent.size()));
     if (!pair_base.empty()) {
         CK(cudaMemcpy(d_pb, pair_base.data(), 8 * pair_base.size(), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(d_pd, pair_doff.data(), 2 * pair_doff.size(), cudaMemcpyHostToDevice));
     }
-    if (s) {
-        CK(cudaMemcpy(d_et, ent_tgt.data(), 2 * s, cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(d_ew, ent_w.data(), 4 * s, cudaMemcpyHostToDevice));
-    }
+    if (!ent.empty()) CK(cudaMemcpy(d_ent, ent.data(), sizeof(uint2) * ent.size(), cudaMemcpyHostToDevice));
     e.a.pair_base = d_pb;
     e.a.pair_doff = d_pd;
-    e.a.ent_tgt = d_et;
-    e.a.ent_w = d_ew;
+    e.a.ent = d_ent;
     return upload_tiles(e, th);
 }
 
@@ -884,7 +936,7 @@ struct TileSeg {
     uint32_t p24, exc24;
     float w_exc, w_inh;
     int32_t d_inst;     // the network's max delay
-    int32_t sign;       // 0: excitatory synapses only (w >= 0), 1: inhibitory only
+    int32_t sign;       // -1: all synapses; 0: excitatory only (w >= 0); 1: inhibitory only
 };
 
 static __device__ __forceinline__ int find_seg(const TileSeg *segs, int n_segs, int64_t k)
@@ -899,11 +951,12 @@ static __device__ __forceinline__ int find_seg(const TileSeg *segs, int n_segs, 
 }
 
 // One warp per (tile, source) pair. Pass 0: per-delay counts -> cumulative
-// pair_doff and pair_cnt. Pass 1: entries in delay order, targets ascending.
+// pair_doff and pair_cnt (each delay's segment padded to even length). Pass 1:
+// entries in delay order, targets ascending.
 template <int PASS>
 __global__ void gen_tile_kernel(const TileSeg *segs, int n_segs, int64_t n_pairs, int D,
                                 int64_t *pair_cnt, uint16_t *pair_doff, const int64_t *pair_base,
-                                uint16_t *ent_tgt, float *ent_w)
+                                uint2 *ent)
 {
     __shared__ long long s_cur[8][GEN_MAX_DELAY];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -920,16 +973,13 @@ __global__ void gen_tile_kernel(const TileSeg *segs, int n_segs, int64_t n_pairs
             SynDraw sd;
             bool conn = j < sg.j1 && draw_pair(sg.pseed, (uint64_t)i, (uint64_t)j, sg.p24, sg.exc24, sg.w_exc,
                                                sg.w_inh, sg.d_inst, &sd);
-            if (conn) conn = (sd.w >= 0.0f) == (sg.sign == 0);
+            if (conn && sg.sign >= 0) conn = (sd.w >= 0.0f) == (sg.sign == 0);
             if (!__ballot_sync(0xffffffffu, conn)) continue;
             const unsigned same = __match_any_sync(0xffffffffu, conn ? sd.d : -1);
             if (conn) {
                 const int leader = __ffs(same) - 1;
                 const long long at = cur[sd.d - 1] + __popc(same & ((1u << lane) - 1u));
-                if (PASS == 1) {
-                    ent_tgt[at] = (uint16_t)(sg.tgt_off + (j - sg.j0));
-                    ent_w[at] = sd.w;
-                }
+                if (PASS == 1) ent[at] = make_uint2((uint32_t)(sg.tgt_off + (j - sg.j0)), __float_as_uint(sd.w));
                 __syncwarp(same);
                 if (lane == leader) cur[sd.d - 1] += __popc(same);
             }
@@ -937,10 +987,11 @@ __global__ void gen_tile_kernel(const TileSeg *segs, int n_segs, int64_t n_pairs
         }
         __syncwarp();
         if (PASS == 0 && lane == 0) {
+            // segments padded to even length (the padding entries are preset)
             long long c = 0;
             for (int d = 0; d <= D; d++) {
                 doff[d] = (uint16_t)c;
-                if (d < D) c += cur[d];
+                if (d < D) c += (cur[d] + 1) & ~1ll;
             }
             pair_cnt[k] = c;
         }
@@ -1164,9 +1215,7 @@ static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, co
         E.a.csc_d = d_cd;
     }
     // target-tiled copy
-    // four 16-bit limbs per sum cannot overflow while every in-degree is < 65,536
-    const bool tiles = wants_tiles(E.opt, D) &&
-                       *std::max_element(maxdeg.begin(), maxdeg.end()) <= 65535ull;
+    const bool tiles = wants_tiles(E.opt, D);
     if (tiles) {
         // target ranges follow population boundaries
         std::vector<int64_t> runs;
@@ -1175,8 +1224,8 @@ static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, co
         runs.push_back(N);
         std::vector<int32_t> tile_beg;
         int32_t tile_max = 0;
-        plan_tiles(runs, auto_tile_size(E.opt, N, E.sm_count), tile_beg, tile_max);
-        const int32_t nu = (int32_t)tile_beg.size() - 1, nt = 2 * nu;
+        plan_tiles(runs, auto_tile_size(E.opt, N, E.sm_count, D), tile_beg, tile_max);
+        const int32_t nu = (int32_t)tile_beg.size() - 1, nt = nu;
         std::vector<TileSeg> segs;
         TileHost th;
         th.n_u = nu;
@@ -1185,8 +1234,10 @@ static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, co
         th.tile_scale.resize(nt);
         th.tile_run_off.assign(nt + 1, 0);
         int64_t pairs = 0;
+        std::vector<int64_t> tile_pair0(nt + 1, 0);
         for (int32_t q = 0; q < nt; q++) {
-            const int32_t qu = q % nu, sign = q / nu;
+            const int32_t qu = q;
+            tile_pair0[q] = pairs;
             int k = 0;
             while (k + 1 < ns && gi[k + 1].nbase <= tile_beg[qu]) k++;
             const GenInst &x = gi[k];
@@ -1213,40 +1264,51 @@ static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, co
                     sg.w_exc = x.w_exc;
                     sg.w_inh = x.w_inh;
                     sg.d_inst = x.D;
-                    sg.sign = sign;
+                    sg.sign = -1;
                     segs.push_back(sg);
                     add_run(th, (uint32_t)sg.src_base, x.n, pairs, D);
                     pairs += x.n;
                 }
             }
         }
+        tile_pair0[nt] = pairs;
         TileSeg *d_segs;
         int64_t *d_pcnt;
         if ((rc = talloc((void **)&d_segs, sizeof(TileSeg) * std::max<size_t>(1, segs.size()))) ||
             (rc = talloc((void **)&d_pcnt, sizeof(int64_t) * (pairs + 1)))) { free_tmp(); return bail(rc); }
         if (!segs.empty()) cudaMemcpy(d_segs, segs.data(), sizeof(TileSeg) * segs.size(), cudaMemcpyHostToDevice);
-        int64_t *d_pb; uint16_t *d_pd, *d_et; float *d_ew;
-        if ((rc = dalloc(E, &d_pb, pairs + 1)) || (rc = dalloc(E, &d_pd, (size_t)pairs * (D + 1))) ||
-            (rc = dalloc(E, &d_et, S)) || (rc = dalloc(E, &d_ew, S))) {
+        int64_t *d_pb; uint16_t *d_pd;
+        if ((rc = dalloc(E, &d_pb, pairs + 1)) || (rc = dalloc(E, &d_pd, (size_t)pairs * (D + 1)))) {
             free_tmp();
             return bail(rc);
         }
         gen_tile_kernel<0><<<gb, 256, 0, E.stream>>>(d_segs, (int)segs.size(), pairs, D, d_pcnt, d_pd, nullptr,
-                                                    nullptr, nullptr);
+                                                    nullptr);
         cudaMemcpyAsync(d_pb, d_pcnt, sizeof(int64_t) * pairs, cudaMemcpyDeviceToDevice, E.stream);
         if ((rc = scan(d_pb, pairs))) { free_tmp(); return bail(rc); }
-        gen_tile_kernel<1><<<gb, 256, 0, E.stream>>>(d_segs, (int)segs.size(), pairs, D, d_pcnt, d_pd, d_pb,
-                                                    d_et, d_ew);
-        int64_t tot = -1;
-        cudaMemcpyAsync(&tot, d_pb + pairs, 8, cudaMemcpyDeviceToHost, E.stream);
-        if (cudaStreamSynchronize(E.stream) != cudaSuccess || tot != S) {
+        int64_t n_ent = 0;
+        cudaMemcpyAsync(&n_ent, d_pb + pairs, 8, cudaMemcpyDeviceToHost, E.stream);
+        if (cudaStreamSynchronize(E.stream) != cudaSuccess) {
             free_tmp();
-            return bail(fail(BSIM_ERR_CUDA, "generator: tiled copy does not match the synapse count"));
+            return bail(fail(BSIM_ERR_CUDA, "generator: tiled copy sizes"));
         }
+        uint2 *d_ent;
+        if ((rc = dalloc(E, &d_ent, n_ent))) { free_tmp(); return bail(rc); }
+        cudaMemsetAsync(d_ent, 0xff, sizeof(uint2) * n_ent, E.stream);  // padding: target 0xffffffff
+        gen_tile_kernel<1><<<gb, 256, 0, E.stream>>>(d_segs, (int)segs.size(), pairs, D, d_pcnt, d_pd, d_pb, d_ent);
+        // entries per tile from the pair offsets at the tiles' first pairs
+        std::vector<int64_t> pb_at(nt + 1, 0);
+        for (int32_t q = 0; q <= nt; q++)
+            cudaMemcpyAsync(&pb_at[q], d_pb + tile_pair0[q], 8, cudaMemcpyDeviceToHost, E.stream);
+        if (cudaStreamSynchronize(E.stream) != cudaSuccess || pb_at[nt] != n_ent) {
+            free_tmp();
+            return bail(fail(BSIM_ERR_CUDA, "generator: tiled copy does not match its sizes"));
+        }
+        E.tile_entries.resize(nt);
+        for (int32_t q = 0; q < nt; q++) E.tile_entries[q] = pb_at[q + 1] - pb_at[q];
         E.a.pair_base = d_pb;
         E.a.pair_doff = d_pd;
-        E.a.ent_tgt = d_et;
-        E.a.ent_w = d_ew;
+        E.a.ent = d_ent;
         if ((rc = upload_tiles(E, th))) { free_tmp(); return bail(rc); }
     }
     // push rows (not needed when every step uses the tiled copy)
@@ -1658,11 +1720,13 @@ __global__ void pop_degree_tiles_kernel(StepArgs a, double *in_sum, double *out_
         for (int r = a.tile_run_off[q]; r < a.tile_run_off[q + 1]; r++) {
             for (int i = threadIdx.x; i < a.run_n[r]; i += blockDim.x) {
                 const int64_t k = a.run_pair0[r] + i;
-                const double c = (double)a.pair_doff[k * (a.D + 1) + a.D];
+                const int64_t b = a.pair_base[k], n_e = a.pair_doff[k * (a.D + 1) + a.D];
+                int64_t real = 0;
+                for (int64_t x = 0; x < n_e; x++) real += a.ent[b + x].x != TILE_PAD;
+                const double c = (double)real;
                 const uint32_t src = a.run_src0[r] + i;
                 if (want_out) atomicAdd(&out_sum[a.ctab[a.cls[src]].pop], c);
-                // tile_beg is indexed by target range: signed tile q covers range q % n_tiles_u
-                if (want_in) atomicAdd(&in_sum[a.ctab[a.cls[a.tile_beg[q % a.n_tiles_u]]].pop], c);
+                if (want_in) atomicAdd(&in_sum[a.ctab[a.cls[a.tile_beg[q]]].pop], c);
             }
         }
     }
@@ -1838,6 +1902,18 @@ int bsim_autotune(bsim_engine *eh, int32_t trial_steps, bsim_tune_result *out)
         out->grid_blocks = e.grid;
         out->delivery = BSIM_DELIVERY_PULL;
         return BSIM_OK;
+    }
+    if (!e.a.acc_clear) {
+        // The trials switch modes, and push adds into the planes: from here on the
+        // LIF phase clears them. The parity the next cycle delivers into holds the
+        // input consumed by the last cycle; zero it (the other parity is unread input).
+        unsigned long long t_next = 0;
+        CK(cudaMemcpy(&t_next, e.a.step_ctr, sizeof(t_next), cudaMemcpyDeviceToHost));
+        const size_t plane_set = (size_t)e.a.n_planes * (size_t)e.N;
+        CK(cudaMemset(reinterpret_cast<longlong2 *>(e.a.acc) + ((t_next & 1ull) ^ 1ull) * plane_set, 0,
+                      sizeof(longlong2) * plane_set));
+        e.a.acc_clear = 1;
+        drop_graph(e);
     }
     std::vector<int> modes;
     if (e.a.row_off) modes.push_back(BSIM_DELIVERY_PUSH);

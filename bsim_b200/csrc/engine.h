@@ -11,6 +11,8 @@
 
 namespace bsim {
 
+constexpr uint32_t TILE_PAD = 0xffffffffu;  // target of a padding entry of the tiled copy
+
 // One neuron class. For LIF_brian neurons: a folded parameter tuple, the
 // per-population part of LIFENeuron::reset's output (src/neuron/lif/LIFENeuron.cpp:68-112);
 // v_tmp depends on i_offset and is kept per neuron. Input-drive neurons
@@ -60,7 +62,10 @@ struct StepArgs {
     uint64_t input_seed;    // seed of the Poisson neurons' draws
     const uint16_t *cls;       // [N] class of each neuron
     const ClassParams *ctab;   // [n_cls]
-    void *acc;                 // [2][N] longlong2 (EXACT) or float2 (ORDERED): input for the next step
+    void *acc;                 // [2][n_planes][N] longlong2 (EXACT) or [2][N] float2 (ORDERED): input
+                               // for the next step; a target's input is the sum over its planes
+    int32_t n_planes;          // accumulator planes (tiled delivery: one per part of a tile)
+    int32_t acc_clear;         // the LIF phase zeroes the planes it read (0: every cycle overwrites them)
     uint32_t *bitmap;          // [R][W] fired flags of each step in the ring
     int32_t *ring;             // [R][cap] fired ids of each step in the ring
     int32_t *ring_cnt;         // [R]
@@ -84,26 +89,30 @@ struct StepArgs {
     // per-population spike counts of the last hist_len steps (predictor input)
     int32_t *pop_hist;          // [hist_len][n_pops]
     int32_t n_pops, hist_len;
-    // target-tiled delivery (BSIM_DELIVERY_TILE). Target ranges ("tiles") are
-    // summed separately for excitatory and inhibitory synapses: signed tile q
-    // covers range q % n_tiles_u with sign q / n_tiles_u (0: E, 1: I). A signed
-    // tile's sources form runs of consecutive neuron ids; every source of a run
-    // owns one (signed tile, source) pair.
-    int32_t n_tiles;                 // signed tiles = 2 * n_tiles_u (0: no tiled copy)
-    int32_t n_tiles_u;               // target ranges
+    // target-tiled delivery (BSIM_DELIVERY_TILE). A tile is a target range whose
+    // excitatory and inhibitory sums are formed in shared memory. Its sources form
+    // runs of consecutive neuron ids; every source of a run owns one (tile, source)
+    // pair. A tile's work units are split into n_planes parts, handed to blocks by a
+    // per-cycle queue; part k stores its sums into accumulator plane k.
+    int32_t n_tiles;                 // tiles (0: no tiled copy)
+    int32_t n_tiles_u;               // = n_tiles (target ranges)
+    int32_t n_parts;                 // = n_tiles * n_planes
+    const int4 *parts;               // [n_parts] {tile, first unit, end unit, plane}, largest first
+    unsigned int *part_ctr;          // next part to hand out (reset by the last block of a cycle)
     int32_t tile_max;                // largest range (neurons): shared-memory accumulator size
-    const int32_t *tile_beg;         // [n_tiles_u + 1] first target of each range
+    const int32_t *tile_beg;         // [n_tiles + 1] first target of each tile
     const float *tile_scale;         // [n_tiles] 2^qexp of the tile's network
-    const int32_t *tile_run_off;     // [n_tiles + 1] range of runs (signed tiles)
+    const int32_t *tile_run_off;     // [n_tiles + 1] range of runs
     const int32_t *tile_units;       // [n_tiles] work units: sum over runs of ceil(n/32) * D
     const uint32_t *run_src0;        // [runs] first source
     const int32_t *run_n;            // [runs] sources in the run
     const int64_t *run_pair0;        // [runs] pair of the first source
     const int32_t *run_unit0;        // [runs] first work unit, counted within the tile
     const int64_t *pair_base;        // [P] first entry of each pair
-    const uint16_t *pair_doff;       // [P][D + 1] cumulative entry counts by delay
-    const uint16_t *ent_tgt;         // [S] target, relative to the tile's first neuron
-    const float *ent_w;              // [S] weight
+    const uint16_t *pair_doff;       // [P][D + 1] cumulative entry counts by delay (padded to even)
+    const uint2 *ent;                // [E] {target within the tile, weight bits}; every (pair, delay)
+                                     // segment starts on an even entry and has even length
+                                     // (padding entries have target 0xffffffff)
     // firing predictor (needs pop_hist)
     const float *mlp;                // [BSIM_MLP_PARAMS] (NULL: off)
     const int32_t *pop_size;         // [n_pops]
@@ -140,6 +149,9 @@ struct Engine {
     bool rec_dirty = false;
     // population statistics (device arrays in a: pop_size, pop_indeg, pop_outdeg)
     bool pop_info_ready = false;
+    // tiled copy, host side: synapses and work units per tile (planning the parts)
+    std::vector<int64_t> tile_entries;
+    std::vector<int32_t> tile_units;
 };
 
 }  // namespace bsim

@@ -95,9 +95,16 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
             const ClassParams *c = a.ctab + a.cls[j];
             float inE, inI;
             if (ACC == BSIM_ACC_EXACT) {
-                longlong2 *acc = reinterpret_cast<longlong2 *>(a.acc) + (int64_t)p * a.N;
-                longlong2 q = acc[j];
-                acc[j] = make_longlong2(0, 0);
+                // the target's input is the (two's-complement) sum over the planes
+                longlong2 *acc = reinterpret_cast<longlong2 *>(a.acc) + (int64_t)p * a.n_planes * a.N + j;
+                longlong2 q = acc[0];
+                for (int k = 1; k < a.n_planes; k++) {
+                    const longlong2 r = acc[(int64_t)k * a.N];
+                    q.x = (long long)((unsigned long long)q.x + (unsigned long long)r.x);
+                    q.y = (long long)((unsigned long long)q.y + (unsigned long long)r.y);
+                }
+                if (a.acc_clear)
+                    for (int k = 0; k < a.n_planes; k++) acc[(int64_t)k * a.N] = make_longlong2(0, 0);
                 const float sd = __ldg(&c->scale_down);
                 inE = __fmul_rn(__ll2float_rn(q.x), sd);
                 inI = __fmul_rn(__ll2float_rn(q.y), sd);
@@ -227,7 +234,7 @@ static __device__ __forceinline__ unsigned long long push_phase(const StepArgs &
     const int D = a.D;
     const long long total = s_cum[D];
     unsigned long long ev = 0;
-    unsigned long long *acc = reinterpret_cast<unsigned long long *>(a.acc) + 2 * (int64_t)pw * a.N;
+    unsigned long long *acc = reinterpret_cast<unsigned long long *>(a.acc) + 2 * (int64_t)pw * a.n_planes * a.N;
     const long long n_warps = ((long long)gridDim.x * blockDim.x) >> 5;
     const long long n_chunks = (total + PUSH_CHUNK - 1) / PUSH_CHUNK;
     for (long long ch = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; ch < n_chunks; ch += n_warps) {
@@ -369,7 +376,8 @@ static __device__ __forceinline__ unsigned long long pull_phase(const StepArgs &
                 sE += __shfl_xor_sync(0xffffffffu, sE, o);
                 sI += __shfl_xor_sync(0xffffffffu, sI, o);
             }
-            if (lane == 0) reinterpret_cast<longlong2 *>(a.acc)[(int64_t)pw * a.N + j] = make_longlong2(sE, sI);
+            if (lane == 0)
+                reinterpret_cast<longlong2 *>(a.acc)[(int64_t)pw * a.n_planes * a.N + j] = make_longlong2(sE, sI);
         } else {
             if (lane == 0) reinterpret_cast<float2 *>(a.acc)[(int64_t)pw * a.N + j] = make_float2(fE, fI);
         }
@@ -378,69 +386,95 @@ static __device__ __forceinline__ unsigned long long pull_phase(const StepArgs &
 }
 
 // ---------------------------------------------------------------------------
-// Phase B, tiled: each block owns a contiguous tile of target neurons and one
-// sign (the excitatory or the inhibitory synapses into it) and sums those
-// inputs exactly in shared memory, so no global atomic is issued; the tile's
-// half of each {E, I} accumulator pair is written out once at the end. Tiles
-// follow population boundaries and hold up to a few thousand targets (16 bytes
-// of counters each), so each source's row into a tile stays a long segment.
+// Phase B, tiled: the exact E and I sums of a tile of target neurons are formed
+// in shared memory, so no global atomic is issued. Tiles follow population
+// boundaries and hold up to a few thousand targets (16 bytes of counters each),
+// so each source's row into a tile stays a long segment. A tile's work is cut
+// into n_planes parts; blocks take parts from a per-cycle queue (largest
+// first), and part k of a tile stores its sums into accumulator plane k (the
+// LIF phase adds the planes), so parts never write the same word.
 //
 // The tile's synapses are grouped by (source, delay) and its sources form runs
 // of consecutive ids. A work unit is (run, delay d, 32-source chunk): one lane
 // reads the chunk's word of the fired bitmap of cycle t-d. Each fired
-// (source, delay) names one segment of entries ({u16 target offset, f32
-// weight}); a warp gathers up to TILE_SEGS segments and streams their entries
-// as one flat range, each lane advancing its own segment cursor.
+// (source, delay) names one segment of 8-byte entries ({target offset in the
+// tile, weight bits}), padded to an even length from an even start; a warp
+// gathers up to TILE_SEGS segments and streams them as one flat range of
+// 16-byte entry pairs, each lane advancing its own segment cursor.
 //
-// Exact sums with 32-bit shared atomics: the int64 fixed-point value of each
-// weight is split into four 16-bit limbs added into four u32 counters. A
-// target gets at most its in-degree (< 65,536, checked at build) inputs per
-// cycle, so no counter can overflow, and sum_k (counter_k << 16k) mod 2^64 is
-// the exact two's-complement sum.
+// Exact int64 sums with 32-bit shared atomics: the low word of the fixed-point
+// value is added with an atomic that returns the old word, and the high word
+// plus the carry out of the low word with a second one. After all additions the
+// (high, low) pair is the exact two's-complement sum (additions commute, and
+// every carry is counted once); the fixed-point exponent keeps every sum below
+// 2^61, so the high word cannot overflow.
 // ---------------------------------------------------------------------------
 #define TILE_SEGS 64
+#ifndef TILE_INFLIGHT
+#define TILE_INFLIGHT 4  // 16-byte entry pairs per lane loaded before they are added
+#endif
 
-// Counters are limb-major ([4][tile]: limb k of target i at k * stride + i) so
-// that lanes adding into scattered targets spread over all shared-memory banks.
-static __device__ __forceinline__ void limb_add(unsigned *c, int stride, long long v)
+// Counters are [4][tile]: E low, E high, I low, I high words (word-major, so
+// lanes adding into scattered targets spread over all shared-memory banks).
+static __device__ __forceinline__ void carry_add(unsigned *lo, int T, long long v)
 {
     const unsigned long long u = (unsigned long long)v;
-    atomicAdd(c, (unsigned)(u & 0xFFFFull));
-    atomicAdd(c + stride, (unsigned)((u >> 16) & 0xFFFFull));
-    atomicAdd(c + 2 * stride, (unsigned)((u >> 32) & 0xFFFFull));
-    atomicAdd(c + 3 * stride, (unsigned)(u >> 48));
+    const unsigned l = (unsigned)u, h = (unsigned)(u >> 32);
+    const unsigned old = atomicAdd(lo, l);
+    atomicAdd(lo + T, h + (old + l < old ? 1u : 0u));
 }
 
-static __device__ __forceinline__ long long limb_sum(const unsigned *c, int stride)
+// Two entries at once: both low words first, so the second atomic's latency
+// overlaps the first's (a returned value is waited for only where it is used).
+static __device__ __forceinline__ void carry_add2(unsigned *lo0, long long v0, unsigned *lo1, long long v1, int T)
 {
-    const unsigned long long u = (unsigned long long)c[0] + ((unsigned long long)c[stride] << 16) +
-                                 ((unsigned long long)c[2 * stride] << 32) +
-                                 ((unsigned long long)c[3 * stride] << 48);
-    return (long long)u;
+    const unsigned long long u0 = (unsigned long long)v0, u1 = (unsigned long long)v1;
+    const unsigned l0 = (unsigned)u0, l1 = (unsigned)u1;
+    const unsigned o0 = atomicAdd(lo0, l0);
+    const unsigned o1 = atomicAdd(lo1, l1);
+    atomicAdd(lo0 + T, (unsigned)(u0 >> 32) + (o0 + l0 < o0 ? 1u : 0u));
+    atomicAdd(lo1 + T, (unsigned)(u1 >> 32) + (o1 + l1 < o1 ? 1u : 0u));
+}
+
+static __device__ __forceinline__ long long carry_sum(const unsigned *lo, int T)
+{
+    return (long long)(((unsigned long long)lo[T] << 32) | (unsigned long long)lo[0]);
 }
 
 static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &a, unsigned long long t, int pw,
-                                                                unsigned *s_acc, long long *s_start, int *s_cum)
+                                                                unsigned *s_acc, long long *s_start, int *s_cum,
+                                                                int *s_part)
 {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int D = a.D;
     long long *seg_start = s_start + warp * TILE_SEGS;
     int *seg_cum = s_cum + warp * TILE_SEGS;
     unsigned long long ev = 0;
-    for (int q = blockIdx.x; q < a.n_tiles; q += gridDim.x) {
-        const int qu = q % a.n_tiles_u, sign = q / a.n_tiles_u;
-        const int tb = a.tile_beg[qu], T = a.tile_beg[qu + 1] - tb;
+    for (;;) {
+        if (threadIdx.x == 0) *s_part = (int)atomicAdd(a.part_ctr, 1u);
+        __syncthreads();
+        const int pi = *s_part;
+        __syncthreads();  // every thread has read s_part before it is written again
+        if (pi >= a.n_parts) break;
+        const int4 part = a.parts[pi];  // {tile, first unit, end unit, plane}
+        const int q = part.x, u_end = part.z;
+        const int tb = a.tile_beg[q], T = a.tile_beg[q + 1] - tb;
         for (int i = threadIdx.x; i < 4 * T; i += blockDim.x) s_acc[i] = 0u;
+        if (threadIdx.x == 0) s_part[1] = part.y;
         __syncthreads();
         const float sc = a.tile_scale[q];
         const int r0 = a.tile_run_off[q], r1 = a.tile_run_off[q + 1];
-        const int n_units = a.tile_units[q];
-        for (int ub = warp * 32; ub < n_units; ub += nwarps * 32) {
+        // the block's warps take 32-unit chunks of the part as they become free
+        for (;;) {
+            int ub = 0;
+            if (lane == 0) ub = atomicAdd(&s_part[1], 32);
+            ub = __shfl_sync(0xffffffffu, ub, 0);
+            if (ub >= u_end) break;
             const int u = ub + lane;
             unsigned m = 0;
             int64_t kbase = 0;
             int d = 1;
-            if (u < n_units) {
+            if (u < u_end) {
                 int r = r0;
                 while (r + 1 < r1 && a.run_unit0[r + 1] <= u) r++;
                 const int n_r = a.run_n[r], chunks = (n_r + 31) >> 5;
@@ -477,8 +511,9 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
                     const int64_t k = kbase + b;
                     const uint16_t *doff = a.pair_doff + k * (D + 1);
                     const int e0 = doff[d - 1], e1 = doff[d];
-                    seg_start[excl + i] = a.pair_base[k] + e0;
-                    seg_cum[excl + i] = e1 - e0;  // length for now
+                    // in 16-byte units: segments start on an even entry and have even length
+                    seg_start[excl + i] = (a.pair_base[k] + e0) >> 1;
+                    seg_cum[excl + i] = (e1 - e0) >> 1;  // length for now
                 }
                 __syncwarp();
                 const int nseg = min(total, TILE_SEGS);
@@ -499,27 +534,35 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
                 if (lane < nseg) seg_cum[lane] = c0;
                 if (lane + 32 < nseg) seg_cum[lane + 32] = half + c1;
                 __syncwarp();
-                const int n_ent = seg_cum[nseg - 1];
-                if (lane == 0) ev += (unsigned long long)n_ent;
+                const int n_pairs = seg_cum[nseg - 1];  // 16-byte entry pairs of the round
+                const uint4 *ent2 = reinterpret_cast<const uint4 *>(a.ent);
                 int j = 0;  // this lane's segment cursor (its flat positions only grow)
-                for (int f0 = 0; f0 < n_ent; f0 += 4 * 32) {
-                    uint16_t tg[4];
-                    float wv[4];
+                for (int f0 = 0; f0 < n_pairs; f0 += TILE_INFLIGHT * 32) {
+                    uint4 v[TILE_INFLIGHT];
 #pragma unroll
-                    for (int uu = 0; uu < 4; uu++) {
+                    for (int uu = 0; uu < TILE_INFLIGHT; uu++) {
                         const int f = f0 + uu * 32 + lane;
-                        if (f < n_ent) {
+                        if (f < n_pairs) {
                             while (seg_cum[j] <= f) j++;
-                            const int64_t e = seg_start[j] + (f - (j ? seg_cum[j - 1] : 0));
-                            tg[uu] = __ldcs(a.ent_tgt + e);
-                            wv[uu] = __ldcs(a.ent_w + e);
+                            v[uu] = ld_stream16(ent2 + seg_start[j] + (f - (j ? seg_cum[j - 1] : 0)));
                         }
                     }
 #pragma unroll
-                    for (int uu = 0; uu < 4; uu++) {
-                        if (f0 + uu * 32 + lane < n_ent) {
-                            const long long qv = __float2ll_rn(__fmul_rn(wv[uu], sc));
-                            limb_add(s_acc + (int)tg[uu], T, qv);
+                    for (int uu = 0; uu < TILE_INFLIGHT; uu++) {
+                        if (f0 + uu * 32 + lane < n_pairs) {
+                            // the sign routes the input as LIFENeuron::recv does; padding (only
+                            // ever the second entry of a pair) is skipped
+                            const float w0 = __uint_as_float(v[uu].y), w1 = __uint_as_float(v[uu].w);
+                            unsigned *c0 = s_acc + (w0 >= 0.0f ? 0 : 2 * T) + (int)v[uu].x;
+                            const long long q0 = __float2ll_rn(__fmul_rn(w0, sc));
+                            if (v[uu].z != TILE_PAD) {
+                                carry_add2(c0, q0, s_acc + (w1 >= 0.0f ? 0 : 2 * T) + (int)v[uu].z,
+                                           __float2ll_rn(__fmul_rn(w1, sc)), T);
+                                ev += 2;
+                            } else {
+                                carry_add(c0, T, q0);
+                                ev += 1;
+                            }
                         }
                     }
                 }
@@ -527,10 +570,11 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
             }
         }
         __syncthreads();
-        // this tile's sign half of each target's {E, I} accumulator pair
-        long long *g = reinterpret_cast<long long *>(a.acc) + 2 * ((int64_t)pw * a.N + tb) + sign;
-        for (int i = threadIdx.x; i < T; i += blockDim.x) g[2 * i] = limb_sum(s_acc + i, T);
-        __syncthreads();
+        // this part's plane of the tile's {E, I} accumulator pairs
+        longlong2 *g = reinterpret_cast<longlong2 *>(a.acc) + ((int64_t)pw * a.n_planes + part.w) * a.N + tb;
+        for (int i = threadIdx.x; i < T; i += blockDim.x)
+            g[i] = make_longlong2(carry_sum(s_acc + i, T), carry_sum(s_acc + 2 * T + i, T));
+        // the next part's queue read (two barriers) orders the reuse of s_acc
     }
     return ev;
 }
@@ -653,6 +697,7 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const __grid
     __shared__ PushSeg s_seg[MAX_WARPS * PUSH_CHUNK];
     __shared__ int s_wcnt[64];
     __shared__ unsigned long long s_ev;
+    __shared__ int s_part[2];  // tiled delivery: the block's part, the part's next unit
     // tiled delivery: [4][tile] u32 limb counters (one sign), then per-warp segment lists
     extern __shared__ __align__(16) unsigned long long s_dyn[];
     const unsigned long long t = *reinterpret_cast<volatile unsigned long long *>(a.step_ctr);
@@ -687,7 +732,7 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const __grid
     } else if (tiled) {
         long long *starts = reinterpret_cast<long long *>(s_dyn + 2 * a.tile_max);
         int *cums = reinterpret_cast<int *>(starts + MAX_WARPS * TILE_SEGS);
-        ev = tile_phase(a, t, p ^ 1, reinterpret_cast<unsigned *>(s_dyn), starts, cums);
+        ev = tile_phase(a, t, p ^ 1, reinterpret_cast<unsigned *>(s_dyn), starts, cums, s_part);
     } else {
         ev = pull_phase<ACC>(a, t, p ^ 1);
     }
@@ -710,6 +755,7 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const __grid
                 }
             }
             *a.ticket = 0u;
+            if (a.part_ctr) *a.part_ctr = 0u;
             *a.step_ctr = t + 1;
             __threadfence();
         }

@@ -66,7 +66,7 @@ typedef struct bsim_options {
     int32_t block_threads; /* threads per block of the step kernel (0: autotuned) */
     int32_t grid_blocks;   /* blocks of the step kernel (0: autotuned) */
     int32_t build_tiles;   /* also build the target-tiled copy (forced on for TILE/AUTO) */
-    int32_t tile_size;     /* target neurons per tile (0: chosen from the network size, <= 8192) */
+    int32_t tile_size;     /* target neurons per tile (0: chosen from the network size and delays, <= 5000) */
     int32_t reserved[7];
 } bsim_options;
 
