@@ -553,15 +553,16 @@ static int plan_tiles(const std::vector<int64_t> &run_beg, int64_t tile, std::ve
 
 // 16 bytes of shared counters per target (two words per E and I sum): tiles of
 // <= 5000 targets let two 512-thread blocks share an SM. Every tile scans the
-// fire bitmaps of its sources for each delay, so that cost grows with tiles x D,
-// while more tiles balance the blocks better. Measured on the generator's
-// networks (D = 6: 400 tiles of 2,500 beat 200 of 5,000; D = 50: 200 beat 400):
-// about 2.7 tiles per SM for short delays, 1.35 for long ones.
+// fire bitmaps of its sources for each delay (a cost of tiles x D), while a
+// source's segment into a tile shrinks with the tile. Measured on the
+// generator's networks: ~1,700 targets best at D = 6 (25 and 100 populations of
+// 10,000), >= 5,000 at D = 50; so 1,700 x sqrt(D / 6), and small networks are cut
+// into at least SMs / 2 tiles (the parts split them further).
 static int64_t auto_tile_size(const bsim_options &o, int64_t N, int sm_count, int32_t D)
 {
     if (o.tile_size > 0) return std::min<int64_t>(o.tile_size, 12288);
-    const double per_sm = D <= 8 ? 2.7 : 1.35;
-    const int64_t t = (int64_t)std::ceil((double)N / (per_sm * sm_count));
+    int64_t t = (int64_t)(1700.0 * std::sqrt((double)D / 6.0));
+    t = std::min<int64_t>(t, (2 * N + sm_count - 1) / sm_count);
     return std::max<int64_t>(256, std::min<int64_t>(5000, t));
 }
 
