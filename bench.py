@@ -34,6 +34,9 @@ HBM_FALLBACK_GBS = 6650.0
 BYTES_PER_NEURON_STEP = 52.0   # read/write v, i_E, i_I, refrac (32), v_tmp (4), read+clear E/I input (16)
 BYTES_PER_EVENT = 8.0          # int32 target + fp32 weight of one delivered synapse
 BYTES_PER_SPIKE = 8.0          # fired id written once, read once
+# Delivery mode per workload when --delivery is not given: the fastest measured on
+# a B200 (1e6-neuron network at ~545 Hz: tiled 0.372 ms per cycle, push 0.436 ms).
+DEFAULT_DELIVERY = {"plain_1m": "tile"}
 
 
 def workload(name, seed):
@@ -121,15 +124,16 @@ def measured_hbm_peak():
     return HBM_FALLBACK_GBS, "fallback"
 
 
-def profiled_traffic(config, delivery):
-    """DRAM bytes per launch of the step kernel from the committed ncu summaries,
-    keyed by workload and delivery mode ("plain_1m/push"), if one was captured."""
+def profiled_traffic(config, delivery, alg_bytes):
+    """DRAM bytes per launch of the step kernel: the committed ncu captures give
+    DRAM bytes per algorithmic byte for a workload and delivery mode ("plain_1m/tile"),
+    applied to this run's algorithmic bytes per launch. None if never captured."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(p):
         d = json.load(open(p))
         v = d.get("%s/%s" % (config, delivery))
-        if isinstance(v, dict):
-            return v.get("bytes_per_launch")
+        if isinstance(v, dict) and v.get("dram_bytes_per_alg_byte"):
+            return v["dram_bytes_per_alg_byte"] * alg_bytes
     return None
 
 
@@ -352,7 +356,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=200)
     ap.add_argument("--config", default="plain_1m")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--delivery", default="push", choices=["push", "pull", "tile", "auto"])
+    ap.add_argument("--delivery", default=None, choices=["push", "pull", "tile", "auto"],
+                    help="default: the fastest measured mode of the workload (DEFAULT_DELIVERY)")
     ap.add_argument("--settle", type=int, default=1000,
                     help="untimed cycles run at set-up so the network leaves its start-up transient")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -360,6 +365,8 @@ def main():
                     help="networks in the batched+predicted vs plain comparison (0 skips it)")
     ap.add_argument("--batched-steps", type=int, default=1000)
     args = ap.parse_args()
+    if args.delivery is None:
+        args.delivery = DEFAULT_DELIVERY.get(args.config, "push")
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
     if args.impl == "reference":
@@ -447,7 +454,7 @@ def main():
     alg_bytes = (BYTES_PER_NEURON_STEP * N + BYTES_PER_EVENT * events / args.steps +
                  BYTES_PER_SPIKE * spikes / args.steps)
     achieved = alg_bytes / (ms / args.steps / 1e3) / 1e9
-    traffic = profiled_traffic(args.config, args.delivery)
+    traffic = profiled_traffic(args.config, args.delivery, alg_bytes)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
             if peak_kind == "measured" else "fallback 6.65 TB/s",
