@@ -346,6 +346,83 @@ def batched_vs_plain(n_nets, steps, device):
                          "ns_per_event_push": tune.cost_push[1], "ns_per_event_tile": tune.cost_tile[1]}}
 
 
+def predicted_vs_plain(steps, device, settle=1000, chunk=50):
+    """The predictor-scheduled workload (200 x 10,000 LIF_brian, delays U{1..20}, i_offset
+    under a 10 Hz square wave) run three ways over the same cycles: plain push, plain
+    tiled, and AUTO delivery chosen per cycle by the trained firing predictor with cost
+    models fitted from the plain runs. Spike counts must agree; the report gives each
+    mode's events/s, the predictor's count error and fallback rate."""
+    import torch
+    import bsim_b200 as B
+    from bsim_b200 import predictor as PR
+    from bsim_b200 import workloads as W
+    specs, _ = W.predicted_2m(1)
+    sp = specs[0]
+    half = sp.drive_half_period
+
+    t_train = time.perf_counter()
+    counts, size, indeg = PR.collect(W.predicted_2m(2)[0], 3000, DT, settle=500, opts=B.options(device=device))
+    x, y = PR.features(counts, size, indeg)
+    params, loss = PR.train(x, y, epochs=3, batch=8192, lr=2e-3)
+    t_train = time.perf_counter() - t_train
+
+    def run_mode(deliv, setup=None):
+        eng = B.Engine.generated(specs, DT, opts=B.options(device=device, delivery=deliv, graph_steps=chunk))
+        if setup:
+            setup(eng)
+        eng.run(settle)
+        st = torch.cuda.ExternalStream(eng.stream(), device=device)
+        ev_c, sp_c, ms_c, hi_c = [], [], [], []
+        fc_prev = eng.fire_count().astype(np.int64)
+        done = 0
+        while done < steps:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            i0 = eng.info().events_total
+            e0.record(st)
+            eng.run_async(chunk)
+            e1.record(st)
+            e1.synchronize()
+            eng.sync()
+            ms_c.append(e0.elapsed_time(e1))
+            ev_c.append(eng.info().events_total - i0)
+            fc = eng.fire_count().astype(np.int64)
+            sp_c.append(int((fc - fc_prev).sum()))
+            fc_prev = fc
+            hi_c.append(((settle + done) // half) % 2 == 1)
+            done += chunk
+        stats = eng.predictor_stats() if deliv == B.DELIVERY_AUTO else None
+        eng.close()
+        return np.array(ev_c, np.float64), np.array(sp_c, np.float64), np.array(ms_c), np.array(hi_c), fc_prev, stats
+
+    ev_p, sp_p, ms_p, hi_p, fc_p, _ = run_mode(B.DELIVERY_PUSH)
+    ev_t, sp_t, ms_t, _, fc_t, _ = run_mode(B.DELIVERY_TILE)
+    cost_push = PR.fit_costs(ev_p / chunk, ms_p * 1e6 / chunk)
+    cost_tile = PR.fit_costs(ev_t / chunk, ms_t * 1e6 / chunk)
+
+    def attach(eng):
+        eng.enable_pop_stats(64)
+        eng.set_predictor(params, tolerance=0.3, cost_push=cost_push, cost_tile=cost_tile)
+
+    ev_a, _, ms_a, _, fc_a, st = run_mode(B.DELIVERY_AUTO, attach)
+    rate = sp_p / chunk / (sp.n_pop * sp.pop_size) / DT
+    eps = lambda ev, ms: float(ev.sum() / (ms.sum() / 1e3))
+    ideal = np.minimum(ms_p, ms_t).sum()  # the better fixed mode, chunk by chunk
+    return {"workload": "predicted_2m: 200 x 10,000 LIF_brian, delays U{1..20}, 10 Hz square-wave i_offset; "
+                        "%d cycles after %d settle cycles" % (steps, settle),
+            "rate_hz_low_high": [float(rate[~hi_p].mean()) if (~hi_p).any() else None,
+                                 float(rate[hi_p].mean()) if hi_p.any() else None],
+            "events_per_s": {"push": eps(ev_p, ms_p), "tile": eps(ev_t, ms_t), "auto_predicted": eps(ev_a, ms_a),
+                             "best_fixed_per_chunk": float(ev_p.sum() / (ideal / 1e3))},
+            "ms_per_cycle": {"push": float(ms_p.sum() / steps), "tile": float(ms_t.sum() / steps),
+                             "auto_predicted": float(ms_a.sum() / steps)},
+            "cost_models_ns": {"push": cost_push, "tile": cost_tile, "form": "a + b * events per cycle"},
+            "spike_counts_identical": bool(np.array_equal(fc_p, fc_t) and np.array_equal(fc_p, fc_a)),
+            "predictor": {"train_loss": loss, "train_seconds": t_train, "cycles": int(st.cycles),
+                          "fallbacks": int(st.fallbacks), "fallback_rate": st.fallbacks / max(st.cycles, 1),
+                          "tile_cycles": int(st.tile_cycles),
+                          "rel_count_error": st.abs_err_sum / max(st.actual_sum, 1.0)}}
+
+
 # ---------------------------------------------------------------------------
 # Our arm
 # ---------------------------------------------------------------------------
@@ -364,6 +441,8 @@ def main():
     ap.add_argument("--batched-nets", type=int, default=32,
                     help="networks in the batched+predicted vs plain comparison (0 skips it)")
     ap.add_argument("--batched-steps", type=int, default=1000)
+    ap.add_argument("--predicted-steps", type=int, default=2000,
+                    help="cycles of the predictor-scheduled comparison (0 skips it)")
     args = ap.parse_args()
     if args.delivery is None:
         args.delivery = DEFAULT_DELIVERY.get(args.config, "push")
@@ -470,12 +549,19 @@ def main():
         except Exception as ex:
             cpu = {"value": None, "unit": "events/s", "cores": 1, "kind": "unavailable", "sample": str(ex)}
 
+    eng.close()  # frees the timed network before the comparisons build theirs
     cmp = None
     if rank == 0 and world == 1 and args.batched_nets > 0:
         try:
             cmp = batched_vs_plain(args.batched_nets, args.batched_steps, local)
         except Exception as ex:
             cmp = {"error": str(ex)}
+    pred = None
+    if rank == 0 and world == 1 and args.predicted_steps > 0:
+        try:
+            pred = predicted_vs_plain(args.predicted_steps, local)
+        except Exception as ex:
+            pred = {"error": str(ex)}
 
     if rank == 0:
         line = {"metric": "synaptic events/s", "value": value, "unit": "events/s", "n_gpus": world,
@@ -491,9 +577,9 @@ def main():
                 "events_per_step": events_all / args.steps / world,
                 "mean_rate_hz": spikes_all / n_all / (args.steps * DT),
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
-                "gpu_launches": args.steps, "batched_predicted_vs_plain": cmp}
+                "gpu_launches": args.steps, "batched_predicted_vs_plain": cmp,
+                "predictor_scheduled_vs_plain": pred}
         print(json.dumps(line))
-    eng.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -652,7 +652,9 @@ static __device__ __forceinline__ int auto_delivery(const StepArgs &a, unsigned 
         as = (float)a.ring_cnt[(t - 1) % (unsigned long long)a.R];
     }
     const bool fallback = t < 3 || fabsf(as - ps) > a.pred_tol * fmaxf(ps, 1.0f);
-    const float work = (float)a.D * (fallback ? as * a.mean_outdeg : pe);
+    // events per cycle: the spikes of one cycle times their out-degree is, at steady
+    // activity, what one cycle delivers (its D slots each hold 1/D of those events)
+    const float work = fallback ? as * a.mean_outdeg : pe;
     const int dm = (a.n_tiles > 0 && a.cost_tile_a + a.cost_tile_b * work < a.cost_push_a + a.cost_push_b * work)
                        ? BSIM_DELIVERY_TILE
                        : BSIM_DELIVERY_PUSH;

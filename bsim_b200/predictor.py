@@ -47,3 +47,17 @@ def collect(specs, steps, dt, settle=200, chunk=1000, opts=None):
 def train(x, y, epochs=30, batch=512, lr=2e-3, seed=1):
     """Trains from a deterministic initialisation on the GPU; returns (params, loss)."""
     return mlp_train(mlp_init(seed), x, y, epochs=epochs, batch=batch, lr=lr, seed=seed)
+
+
+def fit_costs(events_per_cycle, ns_per_cycle):
+    """Least-squares cost model of one delivery mode, ns per cycle = a + b * events
+    per cycle, from per-chunk measurements at varied activity (a, b >= 0)."""
+    e = np.asarray(events_per_cycle, np.float64)
+    t = np.asarray(ns_per_cycle, np.float64)
+    A = np.stack([np.ones_like(e), e], 1)
+    (a, b), *_ = np.linalg.lstsq(A, t, rcond=None)
+    if b < 0:
+        a, b = float(t.mean()), 0.0
+    if a < 0:
+        a, b = 0.0, float((e * t).sum() / max((e * e).sum(), 1e-30))
+    return [float(a), float(b)]

@@ -68,10 +68,11 @@ def batched(n_nets=256, seed=1):
 
 def predicted_2m(seed=1):
     """200 populations x 10,000 neurons (2e6 neurons, ~2.4e9 synapses), delays U{1..20}, 2 s,
-    i_offset under a 10 Hz square wave (x60 in the odd 50 ms half periods) so population
-    rates swing between tens of Hz and ~1 kHz."""
-    sp = cuba(200, 10000, 500, 20, seed, i_max=0.8e-9)
-    sp.drive_scale = 60.0
+    i_offset U[0, 2.5 nA) under a 10 Hz square wave (x32, i.e. up to 80 nA, in the odd 50 ms
+    half periods). Calibrated on the GPU at full size: ~5-15 Hz in the low half periods
+    (drifting up slowly), ~800-1,000 Hz in the high ones."""
+    sp = cuba(200, 10000, 500, 20, seed, i_max=2.5e-9)
+    sp.drive_scale = 32.0
     sp.drive_half_period = 500
     return [sp], 20000
 
