@@ -1,0 +1,107 @@
+"""Edge cases of the step against the oracle (EXACT accumulation, every delivery
+mode that applies): no synapses, a single neuron and ragged sizes, the maximum
+delay, every neuron firing every cycle (full fire-ring slots), sources without
+out-synapses and targets without in-synapses."""
+import numpy as np
+import pytest
+
+import bsim_b200 as B
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+DT = np.float32(1e-4)
+LIF = [-0.065, -0.065, -0.065, 0.25e-9, 20e-3, 2e-3, 5e-3, 10e-3, -0.050, 0.0]
+
+
+def lif_params(n, i_offset, refract=2e-3, seed=0):
+    rng = np.random.default_rng(seed)
+    p = np.tile(np.array(LIF, np.float32), (n, 1))
+    p[:, 0] = rng.uniform(-0.065, -0.051, n)
+    p[:, 5] = refract
+    p[:, 9] = i_offset if np.isscalar(i_offset) else np.asarray(i_offset, np.float32)
+    return p
+
+
+def check(params, src, dst, w, d, steps, modes=("push", "pull", "tile"), cap=None):
+    """Runs the network in each delivery mode and compares raster, spike counts,
+    membrane potentials and delivered events with the fixed-point oracle."""
+    n = params.shape[0]
+    src, dst = np.asarray(src, np.int32), np.asarray(dst, np.int32)
+    w, d = np.asarray(w, np.float32), np.asarray(d, np.int32)
+    opts = {"push": dict(), "pull": dict(delivery=B.DELIVERY_PULL), "tile": dict(delivery=B.DELIVERY_TILE)}
+    cap = cap or max(n * steps, 1)
+    ref = None
+    for m in modes:
+        eng = B.Engine.from_arrays(params, src, dst, w, d, DT, opts=B.options(**opts[m]))
+        eng.record(steps, cap)
+        eng.run(steps)
+        ras = eng.raster()
+        if ref is None:
+            q = int(eng.qexp()[0])
+            ref = oracle.run(params, src, dst, w, d, DT, steps, record_steps=steps, acc_mode=oracle.ACC_FIXED,
+                             qexp=q, raster_cap=cap)
+        assert len(ras) == steps
+        for t in range(steps):
+            assert np.array_equal(ras[t], ref["raster"][t]), (m, t)
+        assert np.array_equal(eng.fire_count(), ref["fire_count"]), m
+        assert np.array_equal(eng.state()["v"], ref["final_state"][:, 0]), m
+        assert eng.info().events_total == ref["events_per_step"].sum(), m
+        eng.close()
+    return ref
+
+
+def test_no_synapses():
+    r = check(lif_params(100, np.linspace(0.0, 0.5e-9, 100)), [], [], [], [], 600)
+    assert r["fire_count"].sum() > 0 and r["events_per_step"].sum() == 0
+
+
+@pytest.mark.parametrize("n", [1, 31, 33, 1007])
+def test_ragged_sizes(n):
+    rng = np.random.default_rng(n)
+    params = lif_params(n, rng.uniform(0.1e-9, 0.4e-9, n), seed=n)
+    s = 4 * n
+    src, dst = rng.integers(0, n, s), rng.integers(0, n, s)
+    w = rng.uniform(-2e-10, 3e-10, s)
+    d = rng.integers(1, 7, s)
+    check(params, src, dst, w, d, 400)
+
+
+def test_max_delay():
+    """A spike fired at cycle t arrives through a delay of BSIM_MAX_DELAY steps (push only:
+    pull takes delays up to 256 and the tiled copy up to 64)."""
+    params = lif_params(3, [0.4e-9, 0.0, 0.0], refract=0.05)
+    d = B.MAX_DELAY
+    r = check(params, [0, 0], [1, 2], [5e-8, 5e-8], [d, 3], d + 200, modes=("push",))
+    fired0 = [t for t, ids in enumerate(r["raster"]) if 0 in ids]
+    fired1 = [t for t, ids in enumerate(r["raster"]) if 1 in ids]
+    # delivered in the synapse phase of t + d, added to i_E by the update of t + d + 1,
+    # seen by v in the update of t + d + 2 (as for the 3-step synapse into neuron 2)
+    fired2 = [t for t, ids in enumerate(r["raster"]) if 2 in ids]
+    assert fired0 and fired1 and fired1[0] == fired0[0] + d + 2 and fired2[0] == fired0[0] + 3 + 2
+
+
+def test_every_neuron_fires_every_cycle():
+    """No refractory period and a suprathreshold drive: all N ids in every ring slot,
+    all-to-all synapses, so each cycle delivers N * N events."""
+    n = 300
+    params = lif_params(n, 60e-9, refract=0.0)  # v_tmp ~ 15 mV per cycle: reset to threshold in one step
+    params[:, 0] = -0.049
+    k = np.arange(n * n)
+    src, dst = k // n, k % n
+    w = np.where(k % 5 == 0, -1e-11, 2e-11)
+    r = check(params, src, dst, w, np.full(n * n, 2), 60)
+    assert r["fire_count"].min() == 60
+
+
+def test_silent_sources_and_unreached_targets():
+    """Half the neurons have no out-synapses, a quarter none in."""
+    n = 800
+    rng = np.random.default_rng(5)
+    params = lif_params(n, rng.uniform(0.0, 0.4e-9, n), seed=5)
+    s = 6000
+    src = rng.integers(0, n // 2, s)
+    dst = rng.integers(n // 4, n, s)
+    w = rng.uniform(-3e-10, 4e-10, s)
+    d = rng.integers(1, 9, s)
+    r = check(params, src, dst, w, d, 500)
+    assert r["fire_count"][: n // 4].sum() > 0
