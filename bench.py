@@ -194,7 +194,8 @@ def cpu_baseline(spec, steps, budget_s=20.0):
         oracle.run(g["params"], g["src"], g["dst"], g["weight"], g["delay_steps"], np.float32(DT), steps)
         secs, kind = time.perf_counter() - t0, "port"
     sample = ("%s: %d steps of a %d x %d replica (%d synapses) of the same generator; 1 thread; "
-              "events/s is independent of the replica size at a fixed rate" %
+              "a replica of the same rates and out-degrees; smaller replicas fit the CPU caches better, so "
+              "this is an upper bound on the full-size network's rate" %
               ("reference STSim float build (oracle/_ref)" if kind == "reference" else "oracle port",
                steps, rs.n_pop, rs.pop_size, len(g["src"])))
     return events / secs, dict(kind=kind, sample=sample, seconds=secs, events=events,
