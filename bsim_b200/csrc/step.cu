@@ -536,15 +536,23 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
                 __syncwarp();
                 const int n_pairs = seg_cum[nseg - 1];  // 16-byte entry pairs of the round
                 const uint4 *ent2 = reinterpret_cast<const uint4 *>(a.ent);
-                int j = 0;  // this lane's segment cursor (its flat positions only grow)
+                // this lane's segment cursor (its flat positions only grow): the current
+                // segment's end, its first flat position and its first entry pair, in registers
+                int j = 0, seg_end = seg_cum[0], seg_first = 0;
+                long long seg_base = seg_start[0];
                 for (int f0 = 0; f0 < n_pairs; f0 += TILE_INFLIGHT * 32) {
                     uint4 v[TILE_INFLIGHT];
 #pragma unroll
                     for (int uu = 0; uu < TILE_INFLIGHT; uu++) {
                         const int f = f0 + uu * 32 + lane;
                         if (f < n_pairs) {
-                            while (seg_cum[j] <= f) j++;
-                            v[uu] = ld_stream16(ent2 + seg_start[j] + (f - (j ? seg_cum[j - 1] : 0)));
+                            while (seg_end <= f) {
+                                seg_first = seg_end;
+                                j++;
+                                seg_end = seg_cum[j];
+                                seg_base = seg_start[j];
+                            }
+                            v[uu] = ld_stream16(ent2 + seg_base + (f - seg_first));
                         }
                     }
 #pragma unroll
