@@ -638,6 +638,29 @@ static int upload_tiles(Engine &e, const TileHost &th)
     return BSIM_OK;
 }
 
+// Segment starts of every (pair, delay) in 16-byte entry pairs, from the pair
+// offsets and the per-delay cumulative counts (all even).
+__global__ void pair_seg_kernel(const int64_t *pair_base, const uint16_t *pair_doff, int64_t n_pairs, int D,
+                                uint32_t *pair_seg)
+{
+    const int64_t n = n_pairs * (D + 1);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        pair_seg[i] = (uint32_t)((pair_base[i / (D + 1)] + pair_doff[i]) >> 1);
+}
+
+static int make_pair_seg(Engine &e, int64_t n_pairs, int64_t n_entries)
+{
+    if (n_entries / 2 > (int64_t)UINT32_MAX) return fail(BSIM_ERR_LIMIT, "tiled delivery: more than 2^33 entries");
+    uint32_t *d_seg;
+    TRY(dalloc(e, &d_seg, (size_t)n_pairs * (e.D + 1)));
+    if (n_pairs > 0)
+        pair_seg_kernel<<<e.sm_count * 4, 256, 0, e.stream>>>(e.a.pair_base, e.a.pair_doff, n_pairs, e.D, d_seg);
+    CK(cudaStreamSynchronize(e.stream));
+    CK(cudaGetLastError());
+    e.a.pair_seg = d_seg;
+    return BSIM_OK;
+}
+
 // Host construction of the tiled copy: target ranges follow population (and
 // network) boundaries; synapses sorted by (tile of the target, source, delay);
 // one pair per distinct (tile, source), runs of consecutive sources.
@@ -750,6 +773,7 @@ static int build_tiles_host(Engine &e, const int32_t *inst, const int32_t *pop, 
     e.a.pair_base = d_pb;
     e.a.pair_doff = d_pd;
     e.a.ent = d_ent;
+    TRY(make_pair_seg(e, (int64_t)pair_base.size(), (int64_t)ent.size()));
     return upload_tiles(e, th);
 }
 
@@ -1310,6 +1334,7 @@ static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, co
         E.a.pair_base = d_pb;
         E.a.pair_doff = d_pd;
         E.a.ent = d_ent;
+        if ((rc = make_pair_seg(E, pairs, n_ent))) { free_tmp(); return bail(rc); }
         if ((rc = upload_tiles(E, th))) { free_tmp(); return bail(rc); }
     }
     // push rows (not needed when every step uses the tiled copy)

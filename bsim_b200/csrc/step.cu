@@ -508,12 +508,11 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
                 for (int i = 0; i < take; i++) {
                     const int b = __ffs(m) - 1;
                     m &= m - 1;
-                    const int64_t k = kbase + b;
-                    const uint16_t *doff = a.pair_doff + k * (D + 1);
-                    const int e0 = doff[d - 1], e1 = doff[d];
                     // in 16-byte units: segments start on an even entry and have even length
-                    seg_start[excl + i] = (a.pair_base[k] + e0) >> 1;
-                    seg_cum[excl + i] = (e1 - e0) >> 1;  // length for now
+                    const uint32_t *ps = a.pair_seg + (kbase + b) * (D + 1) + (d - 1);
+                    const uint32_t s0 = ps[0], s1 = ps[1];
+                    seg_start[excl + i] = s0;
+                    seg_cum[excl + i] = (int)(s1 - s0);  // length for now
                 }
                 __syncwarp();
                 const int nseg = min(total, TILE_SEGS);
