@@ -288,15 +288,16 @@ class Engine:
         _check(lib().bsim_record(self._h, max_steps, capacity))
 
     def raster(self):
-        """Recorded spikes: list of int32 arrays (ascending ids), one per recorded step."""
+        """Recorded spikes: list of int32 arrays (ascending ids), one per recorded step.
+        The arrays are views into one buffer read in a single copy from the device."""
         info = self.info()
         off = np.zeros(info.steps_done + 2, np.int64)
         ns = ctypes.c_int64()
         _check(lib().bsim_read_raster(self._h, _p(off), None, 0, ctypes.byref(ns)))
         total = int(off[ns.value])
-        ids = np.zeros(max(total, 1), np.int32)
+        ids = np.empty(max(total, 1), np.int32)
         _check(lib().bsim_read_raster(self._h, _p(off), _p(ids), ids.shape[0], ctypes.byref(ns)))
-        return [ids[off[k]:off[k + 1]].copy() for k in range(ns.value)]
+        return [ids[off[k]:off[k + 1]] for k in range(ns.value)]
 
     def state(self):
         n = self.info().n_neurons
