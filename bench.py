@@ -268,10 +268,31 @@ def batched_vs_plain(n_nets, steps, device):
     groups = {}
     for i, sp in enumerate(specs):
         groups.setdefault(sp.max_delay, []).append(i)
+    def build_all(tiles):
+        built = []
+        try:
+            for dmax, idx in sorted(groups.items()):
+                built.append((idx, B.Engine.generated(
+                    [specs[i] for i in idx], DT, opts=B.options(device=device, graph_steps=100,
+                                                                delivery=B.DELIVERY_AUTO,
+                                                                build_tiles=0 if tiles else -1))))
+        except B.BsimError:
+            for _, e in built:
+                e.close()
+            raise
+        return built
+
+    tiled_copy = True
+    try:
+        built = build_all(True)
+    except B.BsimError as ex:
+        if ex.code not in (-5, -7):  # BSIM_ERR_NOMEM, BSIM_ERR_LIMIT
+            raise
+        # too large for tiled copies beside the push rows: AUTO then pushes every cycle
+        tiled_copy = False
+        built = build_all(False)
     engines = []
-    for dmax, idx in sorted(groups.items()):
-        eb = B.Engine.generated([specs[i] for i in idx], DT,
-                                opts=B.options(device=device, graph_steps=100, delivery=B.DELIVERY_AUTO))
+    for idx, eb in built:
         eb.run(200)  # past the start-up transient, so that the trials see settled activity
         tune = eb.autotune(10)
         eb.enable_pop_stats(64)
@@ -339,6 +360,7 @@ def batched_vs_plain(n_nets, steps, device):
             "plain_network_seconds_per_s": steps * 1e-4 * n_nets / (plain_ms / 1e3),
             "batched_network_seconds_per_s": steps * 1e-4 * n_nets / (ms_b / 1e3),
             "batched_engines": len(engines), "batched_timing": "wall clock around all engines' cycles",
+            "tiled_copy": tiled_copy,
             "spike_counts_identical": same,
             "predictor": {"train_loss": loss, "train_seconds": t_train, "cycles": st.cycles,
                           "fallbacks": st.fallbacks, "tile_cycles": st.tile_cycles,

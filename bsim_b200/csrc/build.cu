@@ -146,6 +146,8 @@ static int init_device(Engine &e, const bsim_options *opt)
     if (e.opt.accumulate == BSIM_ACC_ORDERED || e.opt.delivery == BSIM_DELIVERY_PULL) e.opt.build_pull = 1;
     if (e.opt.accumulate == BSIM_ACC_ORDERED && e.opt.delivery == BSIM_DELIVERY_TILE)
         return fail(BSIM_ERR_ARG, "tiled delivery needs EXACT accumulation");
+    if (e.opt.delivery == BSIM_DELIVERY_TILE && e.opt.build_tiles < 0)
+        return fail(BSIM_ERR_ARG, "tiled delivery needs the tiled copy (build_tiles >= 0)");
     return BSIM_OK;
 }
 
@@ -572,8 +574,8 @@ static int64_t auto_tile_size(const bsim_options &o, int64_t N, int sm_count, in
 
 static bool wants_tiles(const bsim_options &o, int32_t D)
 {
-    return o.accumulate == BSIM_ACC_EXACT && D <= 64 &&
-           (o.build_tiles || o.delivery == BSIM_DELIVERY_TILE || o.delivery == BSIM_DELIVERY_AUTO);
+    return o.accumulate == BSIM_ACC_EXACT && D <= 64 && o.build_tiles >= 0 &&
+           (o.build_tiles > 0 || o.delivery == BSIM_DELIVERY_TILE || o.delivery == BSIM_DELIVERY_AUTO);
 }
 
 // Host-side description of the tiled copy.

@@ -61,11 +61,12 @@ typedef struct bsim_options {
     int32_t device;        /* CUDA device ordinal (the reference hard-codes 0, SingleGPUSimulator.cu:83) */
     int32_t accumulate;    /* BSIM_ACC_* */
     int32_t delivery;      /* BSIM_DELIVERY_* */
-    int32_t build_pull;    /* also build the target-ordered copy (forced on for PULL/AUTO/ORDERED) */
+    int32_t build_pull;    /* also build the target-ordered copy (forced on for PULL and ORDERED) */
     int32_t graph_steps;   /* steps captured per CUDA graph by bsim_run (0: plain launches) */
     int32_t block_threads; /* threads per block of the step kernel (0: autotuned) */
     int32_t grid_blocks;   /* blocks of the step kernel (0: autotuned) */
-    int32_t build_tiles;   /* also build the target-tiled copy (forced on for TILE/AUTO) */
+    int32_t build_tiles;   /* 1: also build the target-tiled copy; 0: only for TILE/AUTO; -1: never
+                              (an AUTO engine then pushes every cycle; saves ~8 B per synapse) */
     int32_t tile_size;     /* target neurons per tile (0: chosen from the network size and delays, <= 5000) */
     int32_t reserved[7];
 } bsim_options;
