@@ -461,7 +461,7 @@ def main():
     ap.add_argument("--settle", type=int, default=1000,
                     help="untimed cycles run at set-up so the network leaves its start-up transient")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--batched-nets", type=int, default=32,
+    ap.add_argument("--batched-nets", type=int, default=128,
                     help="networks in the batched+predicted vs plain comparison (0 skips it)")
     ap.add_argument("--batched-steps", type=int, default=1000)
     ap.add_argument("--predicted-steps", type=int, default=2000,
