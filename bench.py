@@ -137,6 +137,14 @@ def profiled_traffic(config, delivery, alg_bytes):
     return None
 
 
+def roofline_frac(neuron_steps, events, spikes, seconds):
+    """Algorithmic bytes (52 B per neuron-step, 8 B per event, 8 B per spike) per second
+    as a fraction of the measured HBM copy bandwidth."""
+    peak, _ = measured_hbm_peak()
+    alg = BYTES_PER_NEURON_STEP * neuron_steps + BYTES_PER_EVENT * events + BYTES_PER_SPIKE * spikes
+    return alg / max(seconds, 1e-12) / 1e9 / peak
+
+
 def reduce_over_ranks(dist, maxes, sums, device="cpu"):
     """Max over ranks of each value in `maxes` and sum over ranks of each value in
     `sums` (float64). With dist None (one process) the values come back unchanged.
@@ -301,17 +309,20 @@ def batched_vs_plain(n_nets, steps, device):
     warm = max(int(eb.info().steps_done) for _, eb, _ in engines)
     for _, eb, _ in engines:
         eb.run(warm - int(eb.info().steps_done))
-    plain_ms, plain_ev, plain_counts = 0.0, 0, {}
+    plain_ms, plain_ev, plain_spk, plain_counts = 0.0, 0, 0, {}
     for i, sp in enumerate(specs):
         e = B.Engine.generated(sp, DT, opts=B.options(device=device, graph_steps=100))
         e.run(warm)
+        fc0 = e.fire_count().astype(np.int64)
         ms, ev = timed(e, steps)
         plain_ms += ms
         plain_ev += ev
         plain_counts[i] = e.fire_count()
+        plain_spk += int((plain_counts[i] - fc0).sum())
         e.close()
     torch.cuda.synchronize()
     ev0 = sum(eb.info().events_total for _, eb, _ in engines)
+    spk0 = sum(int(eb.fire_count().astype(np.int64).sum()) for _, eb, _ in engines)
     t0 = time.perf_counter()
     for _, eb, _ in engines:
         eb.run_async(steps)
@@ -319,6 +330,7 @@ def batched_vs_plain(n_nets, steps, device):
         eb.sync()
     ms_b = 1e3 * (time.perf_counter() - t0)
     ev_b = sum(eb.info().events_total for _, eb, _ in engines) - ev0
+    spk_b = sum(int(eb.fire_count().astype(np.int64).sum()) for _, eb, _ in engines) - spk0
     same = True
     n_neurons = n_syn = 0
     cyc = fb = tc = 0
@@ -353,10 +365,14 @@ def batched_vs_plain(n_nets, steps, device):
     info.n_neurons, info.n_synapses = n_neurons, n_syn
     plain = plain_ev / (plain_ms / 1e3)
     batched = ev_b / (ms_b / 1e3)
+    n_all = int(info.n_neurons)
     return {"workload": "%d networks of the batched generator (seed 7), %d cycles each after %d warm-up cycles"
                         % (n_nets, steps, warm),
             "neurons": int(info.n_neurons), "synapses": int(info.n_synapses),
             "plain_events_per_s": plain, "batched_predicted_events_per_s": batched, "ratio": batched / plain,
+            "hbm_roofline_frac": {
+                "plain": roofline_frac(n_all * steps, plain_ev, plain_spk, plain_ms / 1e3),
+                "batched_predicted": roofline_frac(n_all * steps, ev_b, spk_b, ms_b / 1e3)},
             "plain_network_seconds_per_s": steps * 1e-4 * n_nets / (plain_ms / 1e3),
             "batched_network_seconds_per_s": steps * 1e-4 * n_nets / (ms_b / 1e3),
             "batched_engines": len(engines), "batched_timing": "wall clock around all engines' cycles",
@@ -427,8 +443,10 @@ def predicted_vs_plain(steps, device, settle=1000, chunk=50):
         eng.set_predictor(params, tolerance=0.3, cost_push=cost_push, cost_tile=cost_tile)
 
     ev_a, _, ms_a, _, fc_a, st = run_mode(B.DELIVERY_AUTO, attach)
-    rate = sp_p / chunk / (sp.n_pop * sp.pop_size) / DT
+    n_net = sp.n_pop * sp.pop_size
+    rate = sp_p / chunk / n_net / DT
     eps = lambda ev, ms: float(ev.sum() / (ms.sum() / 1e3))
+    frac = lambda ev, ms: roofline_frac(n_net * steps, float(ev.sum()), float(sp_p.sum()), float(ms.sum()) / 1e3)
     ideal = np.minimum(ms_p, ms_t).sum()  # the better fixed mode, chunk by chunk
     return {"workload": "predicted_2m: 200 x 10,000 LIF_brian, delays U{1..20}, 10 Hz square-wave i_offset; "
                         "%d cycles after %d settle cycles" % (steps, settle),
@@ -438,6 +456,7 @@ def predicted_vs_plain(steps, device, settle=1000, chunk=50):
                              "best_fixed_per_chunk": float(ev_p.sum() / (ideal / 1e3))},
             "ms_per_cycle": {"push": float(ms_p.sum() / steps), "tile": float(ms_t.sum() / steps),
                              "auto_predicted": float(ms_a.sum() / steps)},
+            "hbm_roofline_frac": {"push": frac(ev_p, ms_p), "tile": frac(ev_t, ms_t), "auto_predicted": frac(ev_a, ms_a)},
             "cost_models_ns": {"push": cost_push, "tile": cost_tile, "form": "a + b * events per cycle"},
             "spike_counts_identical": bool(np.array_equal(fc_p, fc_t) and np.array_equal(fc_p, fc_a)),
             "predictor": {"train_loss": loss, "train_seconds": t_train, "cycles": int(st.cycles),

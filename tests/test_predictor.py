@@ -143,3 +143,38 @@ def test_population_degrees_from_every_synapse_copy(opts):
         want_out += list(np.bincount(pops[g["src"]], minlength=P) / sp.pop_size)
     assert list(size) == want_size
     assert np.allclose(indeg, want_in, rtol=1e-6) and np.allclose(outdeg, want_out, rtol=1e-6)
+
+
+@pytest.mark.gpu
+def test_autotune_of_a_tiled_engine_keeps_dynamics():
+    """A tiled-only engine never clears its accumulator planes; the autotuner's trials
+    switch it to clearing (push adds into the planes) in mid-run. The spikes and state
+    afterwards equal a push engine's over the same cycles."""
+    sp = W.cuba(10, 1000, 500, 6, seed=8)
+    a = B.Engine.generated(sp, DT, opts=B.options(delivery=B.DELIVERY_TILE))
+    b = B.Engine.generated(sp, DT)
+    a.run(150)
+    r = a.autotune(5)
+    assert r.candidates >= 4
+    steps = a.info().steps_done
+    b.run(steps)
+    a.run(300)
+    b.run(300)
+    assert np.array_equal(a.state()["v"], b.state()["v"])
+    assert np.array_equal(a.fire_count(), b.fire_count())
+
+
+@pytest.mark.gpu
+def test_auto_without_tiled_copy_pushes_every_cycle(trained):
+    params, _ = trained
+    sp = driven(5)
+    plain = B.Engine.generated(sp, DT)
+    auto = B.Engine.generated(sp, DT, opts=B.options(delivery=B.DELIVERY_AUTO, build_tiles=-1))
+    auto.enable_pop_stats(64)
+    auto.set_predictor(params, tolerance=0.3, cost_push=[1e6, 1.0], cost_tile=[0.0, 0.0])
+    for e in (plain, auto):
+        e.run(600)
+    assert np.array_equal(plain.state()["v"], auto.state()["v"])
+    assert auto.predictor_stats().tile_cycles == 0
+    with pytest.raises(B.BsimError):
+        B.Engine.generated(sp, DT, opts=B.options(delivery=B.DELIVERY_TILE, build_tiles=-1))
