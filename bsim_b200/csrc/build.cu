@@ -435,8 +435,8 @@ static int create_from_arrays(const float *params, const uint8_t *kind, int64_t 
 #define MAX_PLANES 8  // parts per tile (accumulator planes)
 #endif
 #ifndef MIN_PLANES
-#define MIN_PLANES 2  // even with many tiles: two parts per tile balance the blocks better
-#endif                // (measured: 1e6 neurons -6 %, 2e6 neurons at D = 20 -19 % per cycle)
+#define MIN_PLANES 1  // parts per tile at least (blocks that run out of parts help the others)
+#endif
 
 // Ring, bitmaps, accumulators, counters; launch shape. Shared by both builders.
 static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
@@ -451,17 +451,20 @@ static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
     TRY(dalloc(e, &d_ctab, ctab.size()));
     CK(cudaMemcpy(d_ctab, ctab.data(), sizeof(ClassParams) * ctab.size(), cudaMemcpyHostToDevice));
     a.ctab = d_ctab;
-    // tiled delivery: each tile's work units in n_planes parts, one accumulator
-    // plane per part; about two parts per resident block (occupancy 2 blocks/SM),
-    // at least MIN_PLANES
+    // tiled delivery: each tile's work units in P parts, one accumulator plane per
+    // part plus the help plane; about two parts per resident block (occupancy 2
+    // blocks/SM), at least MIN_PLANES
     a.n_planes = 1;
     a.n_parts = 0;
     a.parts = nullptr;
+    a.part_next = nullptr;
+    a.help_plane = -1;
     if (a.n_tiles > 0) {
         const int nt = a.n_tiles;
         const double want = 4.0 * e.sm_count / nt;
-        a.n_planes = (int32_t)std::max((double)MIN_PLANES, std::min((double)MAX_PLANES, std::floor(want + 0.5)));
-        const int P = a.n_planes;
+        const int P = (int)std::max((double)MIN_PLANES, std::min((double)MAX_PLANES, std::floor(want + 0.5)));
+        a.n_planes = P + 1;  // the parts' planes and the help plane
+        a.help_plane = P;
         std::vector<int4> parts;
         for (int q = 0; q < nt; q++) {
             const int U = q < (int)e.tile_units.size() ? e.tile_units[q] : 0;
@@ -475,9 +478,15 @@ static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
             return ex > ey;
         });
         int4 *d_parts;
+        unsigned int *d_next;
+        std::vector<unsigned int> next(parts.size());
+        for (size_t i = 0; i < parts.size(); i++) next[i] = (unsigned)parts[i].y;
         TRY(dalloc(e, &d_parts, parts.size()));
+        TRY(dalloc(e, &d_next, parts.size()));
         CK(cudaMemcpy(d_parts, parts.data(), sizeof(int4) * parts.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d_next, next.data(), sizeof(unsigned int) * parts.size(), cudaMemcpyHostToDevice));
         a.parts = d_parts;
+        a.part_next = d_next;
         a.n_parts = (int32_t)parts.size();
     }
     const size_t acc_elem = e.opt.accumulate == BSIM_ACC_ORDERED ? sizeof(float2) : sizeof(longlong2);

@@ -93,12 +93,17 @@ struct StepArgs {
     // excitatory and inhibitory sums are formed in shared memory. Its sources form
     // runs of consecutive neuron ids; every source of a run owns one (tile, source)
     // pair. A tile's work units are split into n_planes parts, handed to blocks by a
-    // per-cycle queue; part k stores its sums into accumulator plane k.
+    // per-cycle queue; part k stores its sums into accumulator plane k. A block that
+    // finds the queue empty joins the part with the most units left and adds its sums
+    // into the help plane (reduction atomics; the LIF phase reads and clears it).
     int32_t n_tiles;                 // tiles (0: no tiled copy)
     int32_t n_tiles_u;               // = n_tiles (target ranges)
     int32_t n_parts;                 // = n_tiles * n_planes
     const int4 *parts;               // [n_parts] {tile, first unit, end unit, plane}, largest first
     unsigned int *part_ctr;          // next part to hand out (reset by the last block of a cycle)
+    unsigned int *part_next;         // [n_parts] next unit of each part: any block may take chunks
+                                     // of any part (reset to the first unit by the last block)
+    int32_t help_plane;              // plane blocks that join another block's part add into (-1: none)
     int32_t tile_max;                // largest range (neurons): shared-memory accumulator size
     const int32_t *tile_beg;         // [n_tiles + 1] first target of each tile
     const float *tile_scale;         // [n_tiles] 2^qexp of the tile's network

@@ -105,6 +105,8 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
                 }
                 if (a.acc_clear)
                     for (int k = 0; k < a.n_planes; k++) acc[(int64_t)k * a.N] = make_longlong2(0, 0);
+                else if (a.help_plane >= 0)
+                    acc[(int64_t)a.help_plane * a.N] = make_longlong2(0, 0);
                 const float sd = __ldg(&c->scale_down);
                 inE = __fmul_rn(__ll2float_rn(q.x), sd);
                 inI = __fmul_rn(__ll2float_rn(q.y), sd);
@@ -450,24 +452,49 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
     long long *seg_start = s_start + warp * TILE_SEGS;
     int *seg_cum = s_cum + warp * TILE_SEGS;
     unsigned long long ev = 0;
+    unsigned long long *s_best = reinterpret_cast<unsigned long long *>(s_part + 2);
     for (;;) {
-        if (threadIdx.x == 0) *s_part = (int)atomicAdd(a.part_ctr, 1u);
+        if (threadIdx.x == 0) {
+            const unsigned q = atomicAdd(a.part_ctr, 1u);
+            s_part[0] = q < (unsigned)a.n_parts ? (int)q : -1;
+            *s_best = 0ull;
+        }
         __syncthreads();
-        const int pi = *s_part;
-        __syncthreads();  // every thread has read s_part before it is written again
-        if (pi >= a.n_parts) break;
+        int pi = s_part[0];
+        const bool helper = pi < 0;
+        if (helper) {
+            // the queue is empty: join the part with the most units left (at least two chunks)
+            unsigned long long best = 0ull;
+            for (int i = threadIdx.x; i < a.n_parts; i += blockDim.x) {
+                const unsigned nx = *reinterpret_cast<volatile unsigned *>(a.part_next + i);
+                const unsigned end = (unsigned)a.parts[i].z;
+                const unsigned left = nx < end ? end - nx : 0u;
+                const unsigned long long key = ((unsigned long long)left << 32) | (unsigned)i;
+                best = key > best ? key : best;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
+                best = other > best ? other : best;
+            }
+            if (lane == 0 && best) atomicMax(s_best, best);
+            __syncthreads();
+            const unsigned long long b = *s_best;
+            pi = (b >> 32) >= 64ull ? (int)(b & 0xffffffffull) : -1;
+        }
+        __syncthreads();  // every thread has read s_part / s_best before they are written again
+        if (pi < 0) break;
         const int4 part = a.parts[pi];  // {tile, first unit, end unit, plane}
         const int q = part.x, u_end = part.z;
         const int tb = a.tile_beg[q], T = a.tile_beg[q + 1] - tb;
         for (int i = threadIdx.x; i < 4 * T; i += blockDim.x) s_acc[i] = 0u;
-        if (threadIdx.x == 0) s_part[1] = part.y;
         __syncthreads();
         const float sc = a.tile_scale[q];
         const int r0 = a.tile_run_off[q], r1 = a.tile_run_off[q + 1];
-        // the block's warps take 32-unit chunks of the part as they become free
+        // the warps of every block working on the part take its 32-unit chunks as they become free
         for (;;) {
             int ub = 0;
-            if (lane == 0) ub = atomicAdd(&s_part[1], 32);
+            if (lane == 0) ub = (int)atomicAdd(a.part_next + pi, 32u);
             ub = __shfl_sync(0xffffffffu, ub, 0);
             if (ub >= u_end) break;
             const int u = ub + lane;
@@ -577,10 +604,21 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
             }
         }
         __syncthreads();
-        // this part's plane of the tile's {E, I} accumulator pairs
-        longlong2 *g = reinterpret_cast<longlong2 *>(a.acc) + ((int64_t)pw * a.n_planes + part.w) * a.N + tb;
-        for (int i = threadIdx.x; i < T; i += blockDim.x)
-            g[i] = make_longlong2(carry_sum(s_acc + i, T), carry_sum(s_acc + 2 * T + i, T));
+        if (!helper) {
+            // the owner stores the part's plane of the tile's {E, I} accumulator pairs
+            longlong2 *g = reinterpret_cast<longlong2 *>(a.acc) + ((int64_t)pw * a.n_planes + part.w) * a.N + tb;
+            for (int i = threadIdx.x; i < T; i += blockDim.x)
+                g[i] = make_longlong2(carry_sum(s_acc + i, T), carry_sum(s_acc + 2 * T + i, T));
+        } else {
+            // a helper adds what it summed into the help plane
+            unsigned long long *g = reinterpret_cast<unsigned long long *>(a.acc) +
+                                    2 * (((int64_t)pw * a.n_planes + a.help_plane) * a.N + tb);
+            for (int i = threadIdx.x; i < T; i += blockDim.x) {
+                const long long e = carry_sum(s_acc + i, T), v = carry_sum(s_acc + 2 * T + i, T);
+                if (e) red_add_u64(g + 2 * i, (unsigned long long)e);
+                if (v) red_add_u64(g + 2 * i + 1, (unsigned long long)v);
+            }
+        }
         // the next part's queue read (two barriers) orders the reuse of s_acc
     }
     return ev;
@@ -706,7 +744,8 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const __grid
     __shared__ PushSeg s_seg[MAX_WARPS * PUSH_CHUNK];
     __shared__ int s_wcnt[64];
     __shared__ unsigned long long s_ev;
-    __shared__ int s_part[2];  // tiled delivery: the block's part, the part's next unit
+    __shared__ __align__(8) int s_part[4];  // tiled delivery: the block's part; [2..3] the best part to join
+    __shared__ int s_last;
     // tiled delivery: [4][tile] u32 limb counters (one sign), then per-warp segment lists
     extern __shared__ __align__(16) unsigned long long s_dyn[];
     const unsigned long long t = *reinterpret_cast<volatile unsigned long long *>(a.step_ctr);
@@ -751,9 +790,15 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const __grid
     if (threadIdx.x == 0) {
         if (s_ev) atomicAdd(a.events, s_ev);
         __threadfence();
-        const unsigned v = atomicAdd(a.ticket, 1u);
-        if (v == gridDim.x - 1) {
-            // every other block has finished this cycle: advance the cycle
+        s_last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (s_last) {
+        // every other block has finished this cycle: the parts' unit counters start over
+        if (tiled)
+            for (int i = threadIdx.x; i < a.n_parts; i += blockDim.x) a.part_next[i] = (unsigned)a.parts[i].y;
+        if (threadIdx.x == 0) {
+            // advance the cycle
             if (a.rec && t > 0) {
                 RecCtl *rc = a.rec;
                 const long long k = (long long)t - 1 - rc->t0;
