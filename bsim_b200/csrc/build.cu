@@ -485,6 +485,10 @@ static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
         TRY(dalloc(e, &d_next, parts.size()));
         CK(cudaMemcpy(d_parts, parts.data(), sizeof(int4) * parts.size(), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(d_next, next.data(), sizeof(unsigned int) * parts.size(), cudaMemcpyHostToDevice));
+        unsigned int *d_help;
+        TRY(dalloc(e, &d_help, parts.size()));
+        CK(cudaMemset(d_help, 0, sizeof(unsigned int) * parts.size()));
+        a.part_help = d_help;
         a.parts = d_parts;
         a.part_next = d_next;
         a.n_parts = (int32_t)parts.size();

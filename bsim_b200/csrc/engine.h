@@ -101,6 +101,7 @@ struct StepArgs {
     int32_t n_parts;                 // = n_tiles * n_planes
     const int4 *parts;               // [n_parts] {tile, first unit, end unit, plane}, largest first
     unsigned int *part_ctr;          // next part to hand out (reset by the last block of a cycle)
+    unsigned int *part_help;         // [n_parts] blocks helping each part this cycle
     unsigned int *part_next;         // [n_parts] next unit of each part: any block may take chunks
                                      // of any part (reset to the first unit by the last block)
     int32_t help_plane;              // plane blocks that join another block's part add into (-1: none)

@@ -463,12 +463,14 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
         int pi = s_part[0];
         const bool helper = pi < 0;
         if (helper) {
-            // the queue is empty: join the part with the most units left (at least two chunks)
+            // the queue is empty: join the part with the most units left per block already
+            // helping it (at least two chunks each), so that helpers spread over the parts
             unsigned long long best = 0ull;
             for (int i = threadIdx.x; i < a.n_parts; i += blockDim.x) {
                 const unsigned nx = *reinterpret_cast<volatile unsigned *>(a.part_next + i);
                 const unsigned end = (unsigned)a.parts[i].z;
-                const unsigned left = nx < end ? end - nx : 0u;
+                const unsigned hp = *reinterpret_cast<volatile unsigned *>(a.part_help + i);
+                const unsigned left = (nx < end ? end - nx : 0u) / (hp + 1u);
                 const unsigned long long key = ((unsigned long long)left << 32) | (unsigned)i;
                 best = key > best ? key : best;
             }
@@ -481,6 +483,7 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
             __syncthreads();
             const unsigned long long b = *s_best;
             pi = (b >> 32) >= 64ull ? (int)(b & 0xffffffffull) : -1;
+            if (pi >= 0 && threadIdx.x == 0) atomicAdd(a.part_help + pi, 1u);
         }
         __syncthreads();  // every thread has read s_part / s_best before they are written again
         if (pi < 0) break;
@@ -796,7 +799,10 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const __grid
     if (s_last) {
         // every other block has finished this cycle: the parts' unit counters start over
         if (tiled)
-            for (int i = threadIdx.x; i < a.n_parts; i += blockDim.x) a.part_next[i] = (unsigned)a.parts[i].y;
+            for (int i = threadIdx.x; i < a.n_parts; i += blockDim.x) {
+                a.part_next[i] = (unsigned)a.parts[i].y;
+                a.part_help[i] = 0u;
+            }
         if (threadIdx.x == 0) {
             // advance the cycle
             if (a.rec && t > 0) {
