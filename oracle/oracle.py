@@ -172,6 +172,26 @@ def ref_available(precision="f32"):
     return os.path.exists(os.path.join(REF_DIR, "ref_driver_" + precision))
 
 
+def run_reference_many(net_path, copies, precision="f32"):
+    """Runs `copies` instances of the reference's own simulator (oracle/_ref) on the
+    same network file at once, one process each, without recording; returns each
+    instance's loop time in seconds (its own timer)."""
+    exe = os.path.join(REF_DIR, "ref_driver_" + precision)
+    d = os.path.dirname(net_path)
+    procs = []
+    for k in range(copies):
+        out = os.path.join(d, "out_%d.bin" % k)
+        procs.append((out, subprocess.Popen([exe, net_path, out, "--no-record"], stdout=subprocess.DEVNULL)))
+    secs = []
+    for out, pr in procs:
+        if pr.wait() != 0:
+            raise RuntimeError("reference driver exited with %d" % pr.returncode)
+        with open(out, "rb") as f:
+            buf = f.read()
+        secs.append(float(np.frombuffer(buf[-8:], dtype=np.float64)[0]))
+    return secs
+
+
 def run_reference(net_path, out_path, precision="f32", record=True, n=None, n_rec=0):
     """Run the reference's own simulator (oracle/_ref) on a network file written by
     tests/netio.write_net; parse its output file."""
