@@ -15,9 +15,10 @@
  *   FireInfo / logFireInfo  src/base/SimInfo.h:19-34, src/base/SimInfo.cpp:4-34
  *   getConstArray / getRandomArray  src/utils/utils.h:34-58
  *
- * Scope: LIF_brian (= IF_curr_exp) neurons with static delayed synapses on one
- * GPU, fp32 (`real` is float; building with USE_DOUBLE is an error). Other
- * neuron types, STSim/MGSim and the multi-GPU path are not provided.
+ * Scope: LIF_brian (= IF_curr_exp) neurons and the Constant_spikes /
+ * Poisson_spikes inputs with static delayed synapses on one GPU, fp32 (`real`
+ * is float; building with USE_DOUBLE is an error). Other neuron types,
+ * STSim/MGSim and the multi-GPU path are not provided.
  *
  * Differences from the reference, by design:
  *   - synapses whose delay rounds to 0 steps make run() fail with -4 (the
@@ -27,7 +28,10 @@
  *   - the single-synapse connect() returns NULL (no per-synapse object exists);
  *   - setting the environment variable BSIM_ACCUMULATE=ordered sums synaptic
  *     input in synapse creation order (bit-identical to the reference CPU
- *     simulator); the default exact int64 accumulation is order-independent.
+ *     simulator); the default exact int64 accumulation is order-independent;
+ *   - BSIM_DELIVERY=tile (or pull) selects the delivery mode (same spikes);
+ *   - Poisson_spikes draw from a generator seeded by BSIM_INPUT_SEED (default 1)
+ *     instead of the clock, so runs are reproducible.
  */
 #ifndef BSIM_B200_BSIM_H
 #define BSIM_B200_BSIM_H
@@ -445,6 +449,9 @@ public:
         bsim_options_default(&opt);
         const char *acc = getenv("BSIM_ACCUMULATE");
         if (acc && strcmp(acc, "ordered") == 0) opt.accumulate = BSIM_ACC_ORDERED;
+        const char *del = getenv("BSIM_DELIVERY");  // push (default), tile or pull
+        if (del && strcmp(del, "tile") == 0) opt.delivery = BSIM_DELIVERY_TILE;
+        if (del && strcmp(del, "pull") == 0) opt.delivery = BSIM_DELIVERY_PULL;
         const int64_t n = (int64_t)pop.size();
         const char *seed_env = getenv("BSIM_INPUT_SEED");
         const uint64_t seed = seed_env ? strtoull(seed_env, NULL, 10) : 1;
