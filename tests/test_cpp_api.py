@@ -47,10 +47,12 @@ def oracle_unit(which):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("which", [1, 2, 3, 4])
-@pytest.mark.parametrize("acc", ["exact", "ordered"])
+@pytest.mark.parametrize("acc", ["exact", "ordered", "exact-tile"])
 def test_sgsim_outputs_match_reference(demos, which, acc):
     ref = oracle_unit(which)
-    env = dict(os.environ, BSIM_ACCUMULATE=acc)
+    env = dict(os.environ, BSIM_ACCUMULATE=acc.split("-")[0])
+    if acc.endswith("tile"):
+        env["BSIM_DELIVERY"] = "tile"
     with tempfile.TemporaryDirectory() as d:
         subprocess.run([demos[1], str(which)], cwd=d, check=True, env=env, stdout=subprocess.DEVNULL)
         count = np.loadtxt(os.path.join(d, "GFire.count"), dtype=np.int64)
