@@ -412,6 +412,12 @@ static __device__ __forceinline__ unsigned long long pull_phase(const StepArgs &
 // 2^61, so the high word cannot overflow.
 // ---------------------------------------------------------------------------
 #define TILE_SEGS 64
+#ifndef TILE_CHUNK_PAIRS
+#define TILE_CHUNK_PAIRS 512  // entry pairs a chunk of units should list (from the previous cycle's rate)
+#endif
+#ifndef TILE_MIN_CHUNK
+#define TILE_MIN_CHUNK 2ll
+#endif
 #ifndef TILE_INFLIGHT
 #define TILE_INFLIGHT 4  // 16-byte entry pairs per lane loaded before they are added
 #endif
@@ -494,17 +500,25 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
         __syncthreads();
         const float sc = a.tile_scale[q];
         const int r0 = a.tile_run_off[q], r1 = a.tile_run_off[q + 1];
-        // the warps of every block working on the part take its 32-unit chunks as they become free
+        // the warps of every block working on the part take chunks of its units as they become
+        // free: 32 units (one per lane), fewer where the part listed many entry pairs per unit in
+        // the previous cycle, so that a hot chunk does not hold up the block for long
+        unsigned *segs_cnt = a.part_segs + (int64_t)(t & 1ull) * a.n_parts + pi;
+        const unsigned prev = a.part_segs[(int64_t)((t & 1ull) ^ 1ull) * a.n_parts + pi];
+        const int cs = prev == 0u ? 32
+                                  : (int)max(TILE_MIN_CHUNK, min(32ll, (long long)TILE_CHUNK_PAIRS * (u_end - part.y) /
+                                                                            (long long)prev));
+        unsigned listed = 0;
         for (;;) {
             int ub = 0;
-            if (lane == 0) ub = (int)atomicAdd(a.part_next + pi, 32u);
+            if (lane == 0) ub = (int)atomicAdd(a.part_next + pi, (unsigned)cs);
             ub = __shfl_sync(0xffffffffu, ub, 0);
             if (ub >= u_end) break;
             const int u = ub + lane;
             unsigned m = 0;
             int64_t kbase = 0;
             int d = 1;
-            if (u < u_end) {
+            if (lane < cs && u < u_end) {
                 int r = r0;
                 while (r + 1 < r1 && a.run_unit0[r + 1] <= u) r++;
                 const int n_r = a.run_n[r], chunks = (n_r + 31) >> 5;
@@ -564,6 +578,7 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
                 if (lane + 32 < nseg) seg_cum[lane + 32] = half + c1;
                 __syncwarp();
                 const int n_pairs = seg_cum[nseg - 1];  // 16-byte entry pairs of the round
+                listed += (unsigned)n_pairs;
                 const uint4 *ent2 = reinterpret_cast<const uint4 *>(a.ent);
                 // this lane's segment cursor (its flat positions only grow): the current
                 // segment's end, its first flat position and its first entry pair, in registers
@@ -606,6 +621,7 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
                 __syncwarp();
             }
         }
+        if (lane == 0 && listed) atomicAdd(segs_cnt, listed);
         __syncthreads();
         if (!helper) {
             // the owner stores the part's plane of the tile's {E, I} accumulator pairs
@@ -802,6 +818,7 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const __grid
             for (int i = threadIdx.x; i < a.n_parts; i += blockDim.x) {
                 a.part_next[i] = (unsigned)a.parts[i].y;
                 a.part_help[i] = 0u;
+                a.part_segs[(int64_t)((t + 1ull) & 1ull) * a.n_parts + i] = 0u;  // written by the next cycle
             }
         if (threadIdx.x == 0) {
             // advance the cycle
