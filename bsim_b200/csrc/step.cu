@@ -416,7 +416,7 @@ static __device__ __forceinline__ unsigned long long pull_phase(const StepArgs &
 #define TILE_CHUNK_PAIRS 512  // entry pairs a chunk of units should list (from the previous cycle's rate)
 #endif
 #ifndef TILE_MIN_CHUNK
-#define TILE_MIN_CHUNK 2ll
+#define TILE_MIN_CHUNK 8ll  // units per chunk at least
 #endif
 #ifndef TILE_INFLIGHT
 #define TILE_INFLIGHT 4  // 16-byte entry pairs per lane loaded before they are added
