@@ -818,8 +818,11 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const __grid
             for (int i = threadIdx.x; i < a.n_parts; i += blockDim.x) {
                 a.part_next[i] = (unsigned)a.parts[i].y;
                 a.part_help[i] = 0u;
-                a.part_segs[(int64_t)((t + 1ull) & 1ull) * a.n_parts + i] = 0u;  // written by the next cycle
             }
+        // the next cycle counts its listed pairs from zero (whichever delivery this cycle used)
+        if (a.part_segs)
+            for (int i = threadIdx.x; i < a.n_parts; i += blockDim.x)
+                a.part_segs[(int64_t)((t + 1ull) & 1ull) * a.n_parts + i] = 0u;
         if (threadIdx.x == 0) {
             // advance the cycle
             if (a.rec && t > 0) {
