@@ -287,15 +287,21 @@ class Engine:
     def record(self, max_steps, capacity):
         _check(lib().bsim_record(self._h, max_steps, capacity))
 
-    def raster(self):
+    def raster(self, out=None):
         """Recorded spikes: list of int32 arrays (ascending ids), one per recorded step.
-        The arrays are views into one buffer read in a single copy from the device."""
+        The arrays are views into one buffer read in a single copy from the device:
+        `out` (a C-contiguous int32 array, e.g. in page-locked memory, reused across
+        reads) when it is large enough, else a new array."""
         info = self.info()
         off = np.zeros(info.steps_done + 2, np.int64)
         ns = ctypes.c_int64()
         _check(lib().bsim_read_raster(self._h, _p(off), None, 0, ctypes.byref(ns)))
         total = int(off[ns.value])
-        ids = np.empty(max(total, 1), np.int32)
+        if (out is not None and out.dtype == np.int32 and out.ndim == 1 and out.flags.c_contiguous
+                and out.shape[0] >= max(total, 1)):
+            ids = out
+        else:
+            ids = np.empty(max(total, 1), np.int32)
         _check(lib().bsim_read_raster(self._h, _p(off), _p(ids), ids.shape[0], ctypes.byref(ns)))
         return [ids[off[k]:off[k + 1]] for k in range(ns.value)]
 

@@ -105,3 +105,29 @@ def test_silent_sources_and_unreached_targets():
     d = rng.integers(1, 9, s)
     r = check(params, src, dst, w, d, 500)
     assert r["fire_count"][: n // 4].sum() > 0
+
+
+def test_raster_into_caller_buffer():
+    """raster(out=...) reads into the caller's buffer (views into it) and gives the same
+    spikes as a fresh read; a buffer too small is not used."""
+    n = 500
+    rng = np.random.default_rng(3)
+    params = lif_params(n, rng.uniform(0.1e-9, 0.4e-9, n), seed=3)
+    s = 3000
+    eng = B.Engine.from_arrays(params, rng.integers(0, n, s).astype(np.int32), rng.integers(0, n, s).astype(np.int32),
+                               rng.uniform(-2e-10, 3e-10, s).astype(np.float32), rng.integers(1, 7, s).astype(np.int32),
+                               DT)
+    eng.record(300, n * 300)
+    eng.run(300)
+    fresh = eng.raster()
+    total = sum(len(r) for r in fresh)
+    assert total > 0
+    buf = np.full(total + 10, -7, np.int32)
+    into = eng.raster(out=buf)
+    assert all(np.array_equal(x, y) for x, y in zip(fresh, into)) and len(into) == len(fresh)
+    assert np.shares_memory(into[-1], buf) or len(into[-1]) == 0
+    assert np.array_equal(buf[:total], np.concatenate(fresh)) and buf[total] == -7
+    small = np.zeros(max(total - 1, 1), np.int32)
+    again = eng.raster(out=small)
+    assert all(np.array_equal(x, y) for x, y in zip(fresh, again)) and not small.any()
+    eng.close()
