@@ -580,14 +580,15 @@ static int plan_tiles(const std::vector<int64_t> &run_beg, int64_t tile, std::ve
 // fire bitmaps of its sources for each delay (a cost of tiles x D), while a
 // source's segment into a tile shrinks with the tile; blocks that run out of
 // parts help the others, so a few hundred tiles balance the GPU. Measured on the
-// generator's networks: ~400 tiles best for 1e6 and 2e6 neurons (2,500 and 5,000
-// targets), ~1,700 targets at D = 6 for smaller ones, >= 5,000 at D = 50: so the
-// larger of N / (2.7 x SMs) and 1,700 x sqrt(D / 6), and small networks are cut
+// generator's networks at their steady rates: ~300 tiles of ~3,300 targets best for
+// 1e6 neurons at D = 6 (7 % faster than 400 of 2,500), 5,000 targets for 2e6
+// neurons, ~1,700 targets at D = 6 for smaller ones, >= 5,000 at D = 50: so the
+// larger of N / (2 x SMs) and 1,700 x sqrt(D / 6), and small networks are cut
 // into at least SMs / 2 tiles (the parts split them further).
 static int64_t auto_tile_size(const bsim_options &o, int64_t N, int sm_count, int32_t D)
 {
     if (o.tile_size > 0) return std::min<int64_t>(o.tile_size, 12288);
-    int64_t t = std::max<int64_t>((int64_t)std::ceil((double)N / (2.7 * sm_count)),
+    int64_t t = std::max<int64_t>((int64_t)std::ceil((double)N / (2.0 * sm_count)),
                                   (int64_t)(1700.0 * std::sqrt((double)D / 6.0)));
     t = std::min<int64_t>(t, (2 * N + sm_count - 1) / sm_count);
     return std::max<int64_t>(256, std::min<int64_t>(5000, t));
