@@ -458,7 +458,7 @@ static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
     a.n_parts = 0;
     a.parts = nullptr;
     a.part_next = nullptr;
-    a.part_segs = nullptr;
+    a.part_pairs = nullptr;
     a.help_plane = -1;
     if (a.n_tiles > 0) {
         const int nt = a.n_tiles;
@@ -490,10 +490,10 @@ static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
         TRY(dalloc(e, &d_help, parts.size()));
         CK(cudaMemset(d_help, 0, sizeof(unsigned int) * parts.size()));
         a.part_help = d_help;
-        unsigned int *d_segs;
-        TRY(dalloc(e, &d_segs, 2 * parts.size()));
-        CK(cudaMemset(d_segs, 0, sizeof(unsigned int) * 2 * parts.size()));
-        a.part_segs = d_segs;
+        unsigned int *d_pairs;
+        TRY(dalloc(e, &d_pairs, 2 * parts.size()));
+        CK(cudaMemset(d_pairs, 0, sizeof(unsigned int) * 2 * parts.size()));
+        a.part_pairs = d_pairs;
         a.parts = d_parts;
         a.part_next = d_next;
         a.n_parts = (int32_t)parts.size();

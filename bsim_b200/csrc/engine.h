@@ -104,7 +104,7 @@ struct StepArgs {
     unsigned int *part_help;         // [n_parts] blocks helping each part this cycle
     unsigned int *part_next;         // [n_parts] next unit of each part: any block may take chunks
                                      // of any part (reset to the first unit by the last block)
-    unsigned int *part_segs;         // [2][n_parts] entry pairs listed per part, by cycle parity;
+    unsigned int *part_pairs;        // [2][n_parts] entry pairs listed per part, by cycle parity;
                                      // the previous cycle's count sizes the part's chunks
     int32_t help_plane;              // plane blocks that join another block's part add into (-1: none)
     int32_t tile_max;                // largest range (neurons): shared-memory accumulator size

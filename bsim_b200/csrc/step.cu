@@ -503,8 +503,8 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
         // the warps of every block working on the part take chunks of its units as they become
         // free: 32 units (one per lane), fewer where the part listed many entry pairs per unit in
         // the previous cycle, so that a hot chunk does not hold up the block for long
-        unsigned *segs_cnt = a.part_segs + (int64_t)(t & 1ull) * a.n_parts + pi;
-        const unsigned prev = a.part_segs[(int64_t)((t & 1ull) ^ 1ull) * a.n_parts + pi];
+        unsigned *pairs_cnt = a.part_pairs + (int64_t)(t & 1ull) * a.n_parts + pi;
+        const unsigned prev = a.part_pairs[(int64_t)((t & 1ull) ^ 1ull) * a.n_parts + pi];
         const int cs = prev == 0u ? 32
                                   : (int)max(TILE_MIN_CHUNK, min(32ll, (long long)TILE_CHUNK_PAIRS * (u_end - part.y) /
                                                                             (long long)prev));
@@ -621,7 +621,7 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
                 __syncwarp();
             }
         }
-        if (lane == 0 && listed) atomicAdd(segs_cnt, listed);
+        if (lane == 0 && listed) atomicAdd(pairs_cnt, listed);
         __syncthreads();
         if (!helper) {
             // the owner stores the part's plane of the tile's {E, I} accumulator pairs
@@ -820,9 +820,9 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const __grid
                 a.part_help[i] = 0u;
             }
         // the next cycle counts its listed pairs from zero (whichever delivery this cycle used)
-        if (a.part_segs)
+        if (a.part_pairs)
             for (int i = threadIdx.x; i < a.n_parts; i += blockDim.x)
-                a.part_segs[(int64_t)((t + 1ull) & 1ull) * a.n_parts + i] = 0u;
+                a.part_pairs[(int64_t)((t + 1ull) & 1ull) * a.n_parts + i] = 0u;
         if (threadIdx.x == 0) {
             // advance the cycle
             if (a.rec && t > 0) {
