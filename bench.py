@@ -572,10 +572,17 @@ def main():
     cap = int(max(4 * spikes, 1024))
     # page-locked host buffers, allocated once outside the timed region as a
     # streaming user would: the state to upload and the raster to read back into
-    pinned = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    def pinned(a):
+        try:
+            return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+        except RuntimeError:  # page-locked memory refused: the pageable copy still works
+            return np.ascontiguousarray(a)
     v, ie, ii, rf = pinned(st["v"]), pinned(st["i_E"]), pinned(st["i_I"]), pinned(st["refrac"])
-    ras_buf = torch.empty(int(1.25 * spikes * e2e_steps / args.steps) + 1024, dtype=torch.int32,
-                          pin_memory=True).numpy()
+    n_ras = int(1.25 * spikes * e2e_steps / args.steps) + 1024
+    try:
+        ras_buf = torch.empty(n_ras, dtype=torch.int32, pin_memory=True).numpy()
+    except RuntimeError:
+        ras_buf = np.empty(n_ras, np.int32)
     eng.record(e2e_steps, cap)  # allocates the recording buffers (drops the captured graph)
     eng.run(100)                # re-captures the graph with recording enabled (not timed)
     eng.record(e2e_steps, cap)  # re-arms the recording only
