@@ -32,6 +32,19 @@ def test_mlp_init_is_deterministic():
     assert np.all(a[576:640] == 0)  # b1
 
 
+def test_fit_costs_linear_model_and_its_guards():
+    """The delivery cost model (ns per cycle = a + b x events) fitted from per-chunk
+    measurements: exact on linear data; a negative slope falls back to the mean cost,
+    a negative intercept to a fit through the origin (both coefficients stay >= 0)."""
+    e = np.array([1e6, 3e6, 7e6, 2e7])
+    assert np.allclose(PR.fit_costs(e, 5e4 + 4e-3 * e), [5e4, 4e-3])
+    a, b = PR.fit_costs(e, 9e4 - 1e-3 * e)
+    assert b == 0.0 and a == pytest.approx((9e4 - 1e-3 * e).mean())
+    t = -2e4 + 6e-3 * e
+    a, b = PR.fit_costs(e, t)
+    assert a == 0.0 and b == pytest.approx((e * t).sum() / (e * e).sum())
+
+
 @pytest.mark.gpu
 def test_mlp_kernels_match_cpu_reference():
     rng = np.random.default_rng(1)
