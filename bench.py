@@ -30,12 +30,12 @@ sys.path.insert(0, ROOT)
 
 DT = 1.0e-4
 HBM_FALLBACK_GBS = 6650.0
-# Algorithmic bytes per unit of work of one step ("Roofline"):
+# Algorithmic bytes per unit of work of one step (the HBM roofline of the path):
 BYTES_PER_NEURON_STEP = 52.0   # read/write v, i_E, i_I, refrac (32), v_tmp (4), read+clear E/I input (16)
 BYTES_PER_EVENT = 8.0          # int32 target + fp32 weight of one delivered synapse
 BYTES_PER_SPIKE = 8.0          # fired id written once, read once
 # Delivery mode per workload when --delivery is not given: the fastest measured on
-# a B200 (1e6-neuron network at ~545 Hz: tiled 0.372 ms per cycle, push 0.436 ms).
+# a B200 (1e6-neuron network at ~545 Hz: tiled 0.223 ms per cycle, push ~0.44 ms).
 DEFAULT_DELIVERY = {"plain_1m": "tile"}
 
 

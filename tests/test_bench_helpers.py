@@ -1,0 +1,49 @@
+"""bench.py's measurement helpers on the CPU: the roofline fraction's algorithmic
+bytes, the traffic estimate from the committed captures, the clock summary's
+parsing of nvidia-smi samples, and the peak lookup's fallback."""
+import json
+import os
+
+import pytest
+
+import bench
+
+
+def test_roofline_fraction_counts_the_algorithmic_bytes(monkeypatch):
+    monkeypatch.setattr(bench, "measured_hbm_peak", lambda: (1000.0, "measured"))
+    # 1e6 neuron-steps x 52 B + 1e8 events x 8 B + 1e5 spikes x 8 B in 1 ms, against 1000 GB/s
+    frac = bench.roofline_frac(1e6, 1e8, 1e5, 1e-3)
+    assert frac == pytest.approx((52e6 + 8e8 + 8e5) / 1e-3 / 1e9 / 1000.0)
+
+
+def test_profiled_traffic_scales_the_captured_ratio():
+    d = json.load(open(os.path.join(bench.ROOT, "profiles", "traffic.json")))
+    r = d["plain_1m/tile"]["dram_bytes_per_alg_byte"]
+    assert 1.0 < r < 3.0
+    assert bench.profiled_traffic("plain_1m", "tile", 5e8) == pytest.approx(r * 5e8)
+    assert bench.profiled_traffic("no_such_workload", "tile", 5e8) is None
+
+
+def test_clock_summary_parses_samples_and_reasons(tmp_path):
+    p = tmp_path / "clocks.csv"
+    p.write_text("0, 1965, 1965, 700.5, 0x0, Not Active, Not Active, Not Active, Not Active\n"
+                 "0, 1950, 1965, 812.0, 0x4, Not Active, Not Active, Not Active, Active\n"
+                 "0, 1965, 1965, 790.0, 0x0, Not Active, Not Active, Not Active, Not Active\n")
+    cs = bench.ClockSampler(0)
+    cs.path = str(p)
+    s = cs.summary()
+    assert s["sm_mhz"] == 1965.0 and s["sm_max_mhz"] == 1965.0 and s["samples"] == 3
+    assert s["reasons"] == ["sw_power_cap"] and s["power_w_max"] == 812.0
+    assert not p.exists()  # the sample file is removed once read
+
+
+def test_clock_summary_without_samples():
+    cs = bench.ClockSampler(0)
+    assert cs.summary()["reasons"] == ["unsampled"]
+
+
+def test_peak_falls_back_without_the_measured_file(monkeypatch, tmp_path):
+    monkeypatch.setattr(bench, "ROOT", str(tmp_path))
+    assert bench.measured_hbm_peak() == (bench.HBM_FALLBACK_GBS, "fallback")
+    (tmp_path / "MEASURED_PEAKS.json").write_text(json.dumps({"hbm_gbs": 6551.0}))
+    assert bench.measured_hbm_peak() == (6551.0, "measured")
