@@ -122,11 +122,14 @@ def generated_net(spec):
 
 
 @needs_ref
-def test_oracle_bit_exact_vs_reference_generated_net():
-    """A 10 x 300 CUBA net with delays U{1..6}: identical rasters, v and spike
-    counts between the restatement and the reference simulator (float build)."""
+@pytest.mark.parametrize("shape", [(10, 300, 100, 6, 5), (8, 250, 2000, 50, 3), (6, 400, 500, 20, 11)])
+def test_oracle_bit_exact_vs_reference_generated_net(shape):
+    """Generated CUBA nets (10 x 300 at 100 Hz with delays U{1..6}; 8 x 250 at 2 kHz
+    with delays U{1..50}; 6 x 400 at 500 Hz with delays U{1..20}): identical rasters,
+    v and spike counts between the restatement and the reference simulator (float build)."""
     from bsim_b200 import workloads as W
-    spec = W.cuba(10, 300, 100, 6, seed=5)
+    n_pop, size, rate, D, seed = shape
+    spec = W.cuba(n_pop, size, rate, D, seed=seed)
     g, net, n = generated_net(spec)
     steps = 400
     rec = np.arange(0, n, 7, dtype=np.int32)
