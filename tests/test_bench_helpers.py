@@ -47,3 +47,18 @@ def test_peak_falls_back_without_the_measured_file(monkeypatch, tmp_path):
     assert bench.measured_hbm_peak() == (bench.HBM_FALLBACK_GBS, "fallback")
     (tmp_path / "MEASURED_PEAKS.json").write_text(json.dumps({"hbm_gbs": 6551.0}))
     assert bench.measured_hbm_peak() == (6551.0, "measured")
+
+
+def test_cpu_baseline_runs_reference_copies_on_a_small_replica():
+    """The CPU baseline and the reference arm: a replica sized to the time budget,
+    `copies` reference processes at once, events summed over the slowest copy."""
+    from oracle import oracle
+    specs, _ = bench.workload("standard_cpu", 1)
+    eps, info = bench.cpu_baseline(specs[0], 20, budget_s=0.2, copies=2)
+    assert eps > 0 and info["seconds"] > 0 and info["events"] > 0
+    if oracle.ref_available("f32"):
+        assert info["kind"] == "reference" and info["copies"] == 2
+        assert eps == pytest.approx(info["events"] / info["seconds"])
+    else:
+        assert info["kind"] == "port" and info["copies"] == 1
+    assert "replica" in info["sample"] and info["replica_synapses"] > 0
