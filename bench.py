@@ -492,6 +492,68 @@ def predicted_vs_plain(steps, device, settle=1000, chunk=50):
 # ---------------------------------------------------------------------------
 # Our arm
 # ---------------------------------------------------------------------------
+def settle(eng, min_steps, max_steps, chunk=250, window=4, tol=0.03):
+    """Runs the network out of its start-up transient before anything is timed: at
+    least min_steps cycles, then chunks of `chunk` cycles until the mean events per
+    cycle of the last `window` chunks is within `tol` of the `window` chunks before
+    them (or max_steps). On the 1e6-neuron network the activity keeps rising for
+    a few thousand cycles after the first spikes, so a fixed short settle would
+    time a transient. Returns the cycles run and the events per cycle of each chunk."""
+    per_chunk = []
+    done = 0
+    while True:
+        e0 = eng.info().events_total
+        eng.run(chunk)
+        done += chunk
+        per_chunk.append((eng.info().events_total - e0) / chunk)
+        if done >= max_steps:
+            break
+        if done >= min_steps and len(per_chunk) >= 2 * window:
+            a = np.mean(per_chunk[-window:])
+            b = np.mean(per_chunk[-2 * window:-window])
+            if abs(a - b) <= tol * max(a, 1.0):
+                break
+    return done, per_chunk
+
+
+def dense_leg(steps, device, settle_min=1000):
+    """The dense-firing configuration (50 x 20,000 LIF_brian, ~2 kHz, delays U{1..50}) as
+    its own device-timed leg: events/s, realtime factor and the HBM roofline of its step."""
+    import torch
+    import bsim_b200 as B
+    specs, desc = workload("dense_1m", 1)
+    deliv = DEFAULT_DELIVERY.get("dense_1m", "push")
+    eng = B.Engine.generated(specs, DT, opts=B.options(device=device, graph_steps=50, delivery={
+        "push": B.DELIVERY_PUSH, "tile": B.DELIVERY_TILE}[deliv]))
+    info = eng.info()
+    N = info.n_neurons
+    settled, _ = settle(eng, settle_min, 4 * settle_min, chunk=250, window=2)
+    eng.run(5)
+    st = torch.cuda.ExternalStream(eng.stream(), device=device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    i0 = eng.info().events_total
+    fc0 = eng.fire_count().astype(np.int64)
+    e0.record(st)
+    eng.run_async(steps)
+    e1.record(st)
+    e1.synchronize()
+    eng.sync()
+    ms = e0.elapsed_time(e1)
+    ev = eng.info().events_total - i0
+    spk = int((eng.fire_count().astype(np.int64) - fc0).sum())
+    eng.close()
+    peak, _ = measured_hbm_peak()
+    alg = BYTES_PER_NEURON_STEP * N + BYTES_PER_EVENT * ev / steps + BYTES_PER_SPIKE * spk / steps
+    ach = alg / (ms / steps / 1e3) / 1e9
+    return {"workload": "dense_1m: " + desc, "neurons": N, "synapses": int(info.n_synapses), "delivery": deliv,
+            "settle_steps": settled, "steps": steps, "ms_per_step": ms / steps, "events_per_s": ev / (ms / 1e3),
+            "events_per_step": ev / steps, "mean_rate_hz": spk / N / (steps * DT),
+            "realtime_factor": steps * DT / (ms / 1e3),
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                         "alg_bytes_per_launch": alg}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -501,8 +563,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--delivery", default=None, choices=["push", "pull", "tile", "auto"],
                     help="default: the fastest measured mode of the workload (DEFAULT_DELIVERY)")
-    ap.add_argument("--settle", type=int, default=1000,
-                    help="untimed cycles run at set-up so the network leaves its start-up transient")
+    ap.add_argument("--settle", type=int, default=3000,
+                    help="untimed cycles run at set-up at least, so the network leaves its start-up transient")
+    ap.add_argument("--settle-max", type=int, default=10000,
+                    help="settling stops here even if the activity is still drifting")
+    ap.add_argument("--dense-steps", type=int, default=200,
+                    help="timed cycles of the dense-firing leg (50 x 20,000, ~2 kHz, delays 1-50; 0 skips it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batched-nets", type=int, default=128,
                     help="networks in the batched+predicted vs plain comparison (0 skips it)")
@@ -539,7 +605,7 @@ def main():
     info = eng.info()
     N, S = info.n_neurons, info.n_synapses
 
-    eng.run(args.settle)   # set-up: leave the start-up transient (rates settle within ~0.1 s)
+    settled = settle(eng, args.settle, args.settle_max)
     eng.run(args.warmup)
     stream = torch.cuda.ExternalStream(eng.stream(), device=local)
     e0 = torch.cuda.Event(enable_timing=True)
@@ -581,8 +647,10 @@ def main():
     n_ras = int(1.25 * spikes * e2e_steps / args.steps) + 1024
     try:
         ras_buf = torch.empty(n_ras, dtype=torch.int32, pin_memory=True).numpy()
+        cnt_buf = torch.empty(N, dtype=torch.int32, pin_memory=True).numpy()
     except RuntimeError:
         ras_buf = np.empty(n_ras, np.int32)
+        cnt_buf = np.empty(N, np.int32)
     eng.record(e2e_steps, cap)  # allocates the recording buffers (drops the captured graph)
     eng.run(100)                # re-captures the graph with recording enabled (not timed)
     eng.record(e2e_steps, cap)  # re-arms the recording only
@@ -592,10 +660,16 @@ def main():
     ia = eng.info()
     t0 = time.perf_counter()
     eng.write_state(v, ie, ii, rf)
+    t1 = time.perf_counter()
     eng.run(e2e_steps)
+    t2 = time.perf_counter()
     raster = eng.raster(out=ras_buf)
-    counts = eng.fire_count()
-    t_e2e = time.perf_counter() - t0
+    t3 = time.perf_counter()
+    counts = eng.fire_count(out=cnt_buf)
+    t4 = time.perf_counter()
+    t_e2e = t4 - t0
+    parts_ms = {"write_state": 1e3 * (t1 - t0), "run": 1e3 * (t2 - t1), "raster": 1e3 * (t3 - t2),
+                "fire_count": 1e3 * (t4 - t3)}
     ib = eng.info()
     ev_e2e = float(ib.events_total - ia.events_total)
     spk_e2e = sum(len(r) for r in raster)
@@ -603,9 +677,11 @@ def main():
     e2e = {"value": ev_all_e2e / t_e2e_max, "unit": "events/s",
            "h2d_bytes_per_step": 16.0 * N / e2e_steps,
            "d2h_bytes_per_step": (4.0 * spk_e2e + 8.0 * (e2e_steps + 1) + 4.0 * len(counts)) / e2e_steps,
-           "realtime_factor": e2e_steps * DT / t_e2e_max,
+           "realtime_factor": e2e_steps * DT / t_e2e_max, "steps": e2e_steps,
+           "parts_ms": parts_ms,
            "path": "bsim_write_state (H2D from page-locked buffers) + bsim_run with spike recording + "
-                   "bsim_read_raster (into a page-locked buffer) + bsim_read_fire_count (D2H), wall clock"}
+                   "bsim_read_raster (into a page-locked buffer) + bsim_read_fire_count (D2H into a "
+                   "page-locked buffer), wall clock, each call synchronous"}
 
     peak, peak_kind = measured_hbm_peak()
     alg_bytes = (BYTES_PER_NEURON_STEP * N + BYTES_PER_EVENT * events / args.steps +
@@ -634,6 +710,12 @@ def main():
             cmp = batched_vs_plain(args.batched_nets, args.batched_steps, local)
         except Exception as ex:
             cmp = {"error": str(ex)}
+    dense = None
+    if rank == 0 and world == 1 and args.dense_steps > 0:
+        try:
+            dense = dense_leg(args.dense_steps, local)
+        except Exception as ex:
+            dense = {"error": str(ex)}
     pred = None
     if rank == 0 and world == 1 and args.predicted_steps > 0:
         try:
@@ -650,12 +732,13 @@ def main():
                            "delivery": args.delivery, "accumulate": "exact int64",
                            "parallelism": "replicas x%d (independent networks, no collective)" % world,
                            "l2": "inputs larger than L2 (%.1f GB of synapse rows per GPU)" % (S * 8 / 1e9),
-                           "build_seconds": t_build, "settle_steps": args.settle},
+                           "build_seconds": t_build, "settle_steps": settled[0],
+                           "settle_events_per_cycle_last_chunks": [float(x) for x in settled[1][-8:]]},
                 "realtime_factor": rtf, "spikes_per_step": spikes_all / args.steps / world,
                 "events_per_step": events_all / args.steps / world,
                 "mean_rate_hz": spikes_all / n_all / (args.steps * DT),
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
-                "gpu_launches": args.steps, "batched_predicted_vs_plain": cmp,
+                "gpu_launches": args.steps, "dense_c2": dense, "batched_predicted_vs_plain": cmp,
                 "predictor_scheduled_vs_plain": pred}
         print(json.dumps(line))
     if dist:

@@ -362,9 +362,15 @@ class Engine:
         _check(lib().bsim_get_stream(self._h, ctypes.byref(s)))
         return s.value or 0
 
-    def fire_count(self):
+    def fire_count(self, out=None):
+        """Spikes per neuron since creation; into `out` (a C-contiguous int32 array of
+        n_neurons, e.g. in page-locked memory, reused across reads) when given."""
         n = self.info().n_neurons
-        c = np.zeros(n, np.int32)
+        if (out is not None and out.dtype == np.int32 and out.ndim == 1 and out.flags.c_contiguous
+                and out.shape[0] == n):
+            c = out
+        else:
+            c = np.zeros(n, np.int32)
         _check(lib().bsim_read_fire_count(self._h, _p(c)))
         return c
 

@@ -1517,7 +1517,13 @@ static int check_err(Engine &e)
 {
     int32_t err = 0;
     CK(cudaMemcpy(&err, e.a.err, 4, cudaMemcpyDeviceToHost));
-    if (err) return fail(BSIM_ERR_DEVICE, "device error flag " + std::to_string(err));
+    if (err) {
+        static const char *names[] = {"", "row offsets not ascending", "synapse target outside the network",
+                                      "class index or kind out of range", "row offsets do not span the synapses"};
+        std::string m = "device error flag " + std::to_string(err);
+        if (err > 0 && err <= 4) m += std::string(" (") + names[err] + ")";
+        return fail(BSIM_ERR_DEVICE, m);
+    }
     return BSIM_OK;
 }
 
@@ -1573,6 +1579,15 @@ int bsim_run(bsim_engine *eh, int64_t steps)
     return bsim_sync(eh);
 }
 
+// Scratch of the per-cycle sort of a recording of `items` ids over `segs` cycles.
+static int sort_scratch_bytes(Engine &e, int64_t items, int64_t segs, size_t *bytes)
+{
+    *bytes = 0;
+    CK(cub::DeviceSegmentedSort::SortKeys(nullptr, *bytes, e.a.rec_ids, e.rec_sorted, (int)std::max<int64_t>(items, 1),
+                                          (int)std::max<int64_t>(segs, 1), e.a.rec_off, e.a.rec_off + 1, e.stream));
+    return BSIM_OK;
+}
+
 int bsim_record(bsim_engine *eh, int64_t max_steps, int64_t capacity)
 {
     if (!eh || max_steps < 0 || capacity < 0) return fail(BSIM_ERR_ARG, "bsim_record: invalid arguments");
@@ -1587,15 +1602,31 @@ int bsim_record(bsim_engine *eh, int64_t max_steps, int64_t capacity)
     }
     if (max_steps > e.rec_steps_alloc || capacity > e.rec_cap_alloc || !e.a.rec_ids) {
         // grow the buffers; the captured graph holds the old pointers
-        int32_t *ids;
+        int32_t *ids, *sorted;
         int64_t *off;
-        TRY(dalloc(e, &ids, std::max<int64_t>(capacity, e.rec_cap_alloc)));
-        TRY(dalloc(e, &off, std::max<int64_t>(max_steps, e.rec_steps_alloc) + 1));
+        const int64_t cap = std::max<int64_t>(capacity, e.rec_cap_alloc);
+        const int64_t stp = std::max<int64_t>(max_steps, e.rec_steps_alloc);
+        TRY(dalloc(e, &ids, cap));
+        TRY(dalloc(e, &off, stp + 1));
         e.a.rec_ids = ids;
         e.a.rec_off = off;
-        e.rec_cap_alloc = std::max<int64_t>(capacity, e.rec_cap_alloc);
-        e.rec_steps_alloc = std::max<int64_t>(max_steps, e.rec_steps_alloc);
+        e.rec_cap_alloc = cap;
+        e.rec_steps_alloc = stp;
         e.rec_dirty = true;
+        // the read-back's sorted copy and sort scratch, sized for a full recording
+        // (recordings of 2^31 ids or more are sorted on the host and need neither)
+        if (cap < ((int64_t)1 << 31) && stp < ((int64_t)1 << 31)) {
+            TRY(dalloc(e, &sorted, cap));
+            e.rec_sorted = sorted;
+            size_t tb = 0;
+            TRY(sort_scratch_bytes(e, cap, stp, &tb));
+            if (tb > e.sort_tmp_bytes) {
+                char *tmp;
+                TRY(dalloc(e, &tmp, tb));
+                e.sort_tmp = tmp;
+                e.sort_tmp_bytes = tb;
+            }
+        }
     }
     RecCtl ctl{e.steps_done, e.steps_done, max_steps, capacity};
     CK(cudaMemset(e.a.rec_off, 0, sizeof(int64_t)));
@@ -1615,9 +1646,9 @@ int bsim_read_raster(bsim_engine *eh, int64_t *step_off, int32_t *ids, int64_t i
     if (!e.a.rec || !e.a.rec_ids) return fail(BSIM_ERR_STATE, "bsim_read_raster: recording not enabled");
     CK(cudaSetDevice(e.device));
     CK(launch_record_flush(e));
-    CK(cudaStreamSynchronize(e.stream));
     RecCtl ctl;
-    CK(cudaMemcpy(&ctl, e.a.rec, sizeof(ctl), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpyAsync(&ctl, e.a.rec, sizeof(ctl), cudaMemcpyDeviceToHost, e.stream));
+    CK(cudaStreamSynchronize(e.stream));
     int64_t ns = ctl.next - ctl.t0;
     if (ns < 0) ns = 0;
     if (ns > ctl.steps) ns = ctl.steps;
@@ -1629,49 +1660,81 @@ int bsim_read_raster(bsim_engine *eh, int64_t *step_off, int32_t *ids, int64_t i
         if (total > ids_cap) return fail(BSIM_ERR_ARG, "bsim_read_raster: ids buffer too small");
         if (total == 0) return BSIM_OK;
         // ascending ids within each cycle: one segmented sort on the device (the
-        // cycles' segments tile the recording); recordings of 2^31 ids or more
-        // are sorted on the host
-        if (total >= ((int64_t)1 << 31) || ns >= ((int64_t)1 << 31)) {
+        // cycles' segments tile the recording) into the buffers bsim_record set up;
+        // recordings of 2^31 ids or more are sorted on the host
+        if (!e.rec_sorted || total >= ((int64_t)1 << 31) || ns >= ((int64_t)1 << 31)) {
             CK(cudaMemcpy(ids, e.a.rec_ids, sizeof(int32_t) * total, cudaMemcpyDeviceToHost));
             for (int64_t k = 0; k < ns; k++) std::sort(ids + step_off[k], ids + step_off[k + 1]);
             return BSIM_OK;
         }
-        int32_t *d_sorted = nullptr;
-        void *d_tmp = nullptr;
         size_t tmp_bytes = 0;
-        cudaError_t st = cub::DeviceSegmentedSort::SortKeys(nullptr, tmp_bytes, e.a.rec_ids, d_sorted, (int)total,
-                                                            (int)ns, e.a.rec_off, e.a.rec_off + 1, e.stream);
-        if (st == cudaSuccess) st = cudaMalloc((void **)&d_sorted, sizeof(int32_t) * total);
-        if (st == cudaSuccess) st = cudaMalloc(&d_tmp, tmp_bytes ? tmp_bytes : 1);
-        if (st == cudaSuccess)
-            st = cub::DeviceSegmentedSort::SortKeys(d_tmp, tmp_bytes, e.a.rec_ids, d_sorted, (int)total, (int)ns,
-                                                    e.a.rec_off, e.a.rec_off + 1, e.stream);
-        if (st == cudaSuccess) st = cudaMemcpyAsync(ids, d_sorted, sizeof(int32_t) * total, cudaMemcpyDeviceToHost, e.stream);
-        if (st == cudaSuccess) st = cudaStreamSynchronize(e.stream);
-        cudaFree(d_tmp);
-        cudaFree(d_sorted);
-        if (st != cudaSuccess) {
-            cudaGetLastError();
-            return fail(BSIM_ERR_CUDA, std::string("bsim_read_raster: ") + cudaGetErrorString(st));
+        TRY(sort_scratch_bytes(e, total, ns, &tmp_bytes));
+        if (tmp_bytes > e.sort_tmp_bytes) {  // not expected: the scratch was sized for a full recording
+            char *tmp;
+            TRY(dalloc(e, &tmp, tmp_bytes));
+            e.sort_tmp = tmp;
+            e.sort_tmp_bytes = tmp_bytes;
         }
+        size_t tb = e.sort_tmp_bytes;
+        CK(cub::DeviceSegmentedSort::SortKeys(e.sort_tmp, tb, e.a.rec_ids, e.rec_sorted, (int)total, (int)ns,
+                                              e.a.rec_off, e.a.rec_off + 1, e.stream));
+        CK(cudaMemcpyAsync(ids, e.rec_sorted, sizeof(int32_t) * total, cudaMemcpyDeviceToHost, e.stream));
+        CK(cudaStreamSynchronize(e.stream));
     }
     return BSIM_OK;
 }
+
+// The state's four fields as planes of N words in the staging buffer (read-back),
+// and back (upload; a NULL plane leaves its field).
+__global__ void state_unpack_kernel(const float4 *st, float *stage, int64_t n)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float4 s = st[i];
+        stage[i] = s.x;
+        stage[n + i] = s.y;
+        stage[2 * n + i] = s.z;
+        stage[3 * n + i] = s.w;
+    }
+}
+
+__global__ void state_pack_kernel(float4 *st, const float *stage, int64_t n, int has_v, int has_ie, int has_ii,
+                                  int has_rf)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float4 s = st[i];
+        if (has_v) s.x = stage[i];
+        if (has_ie) s.y = stage[n + i];
+        if (has_ii) s.z = stage[2 * n + i];
+        if (has_rf) s.w = stage[3 * n + i];
+        st[i] = s;
+    }
+}
+
+static int ensure_stage(Engine &e)
+{
+    if (e.stage) return BSIM_OK;
+    float *d;
+    TRY(dalloc(e, &d, 4 * (size_t)e.N));
+    e.stage = d;
+    return BSIM_OK;
+}
+
+static int state_grid(const Engine &e) { return (int)std::min<int64_t>((e.N + 255) / 256, 8 * (int64_t)e.sm_count); }
 
 int bsim_read_state(bsim_engine *eh, float *v, float *iE, float *iI, int32_t *refrac)
 {
     if (!eh) return fail(BSIM_ERR_ARG, "null engine");
     Engine &e = *H(eh);
     CK(cudaSetDevice(e.device));
+    TRY(ensure_stage(e));
+    state_unpack_kernel<<<state_grid(e), 256, 0, e.stream>>>(e.a.state, e.stage, e.N);
+    CK(cudaGetLastError());
+    void *dst[4] = {v, iE, iI, refrac};
+    for (int k = 0; k < 4; k++)
+        if (dst[k])
+            CK(cudaMemcpyAsync(dst[k], e.stage + (size_t)k * e.N, sizeof(float) * e.N, cudaMemcpyDeviceToHost,
+                               e.stream));
     CK(cudaStreamSynchronize(e.stream));
-    std::vector<float4> st(e.N);
-    CK(cudaMemcpy(st.data(), e.a.state, sizeof(float4) * e.N, cudaMemcpyDeviceToHost));
-    for (int64_t i = 0; i < e.N; i++) {
-        if (v) v[i] = st[i].x;
-        if (iE) iE[i] = st[i].y;
-        if (iI) iI[i] = st[i].z;
-        if (refrac) memcpy(&refrac[i], &st[i].w, 4);
-    }
     return BSIM_OK;
 }
 
@@ -1680,17 +1743,16 @@ int bsim_write_state(bsim_engine *eh, const float *v, const float *iE, const flo
     if (!eh) return fail(BSIM_ERR_ARG, "null engine");
     Engine &e = *H(eh);
     CK(cudaSetDevice(e.device));
+    TRY(ensure_stage(e));
+    const void *src[4] = {v, iE, iI, refrac};
+    for (int k = 0; k < 4; k++)
+        if (src[k])
+            CK(cudaMemcpyAsync(e.stage + (size_t)k * e.N, src[k], sizeof(float) * e.N, cudaMemcpyHostToDevice,
+                               e.stream));
+    state_pack_kernel<<<state_grid(e), 256, 0, e.stream>>>(e.a.state, e.stage, e.N, v != nullptr, iE != nullptr,
+                                                            iI != nullptr, refrac != nullptr);
+    CK(cudaGetLastError());
     CK(cudaStreamSynchronize(e.stream));
-    std::vector<float4> st(e.N);
-    if (!(v && iE && iI && refrac))  // partial update: keep the other fields
-        CK(cudaMemcpy(st.data(), e.a.state, sizeof(float4) * e.N, cudaMemcpyDeviceToHost));
-    for (int64_t i = 0; i < e.N; i++) {
-        if (v) st[i].x = v[i];
-        if (iE) st[i].y = iE[i];
-        if (iI) st[i].z = iI[i];
-        if (refrac) memcpy(&st[i].w, &refrac[i], 4);
-    }
-    CK(cudaMemcpy(e.a.state, st.data(), sizeof(float4) * e.N, cudaMemcpyHostToDevice));
     return BSIM_OK;
 }
 
@@ -1730,8 +1792,8 @@ int bsim_read_fire_count(bsim_engine *eh, int32_t *count)
     if (!eh || !count) return fail(BSIM_ERR_ARG, "invalid arguments");
     Engine &e = *H(eh);
     CK(cudaSetDevice(e.device));
+    CK(cudaMemcpyAsync(count, e.a.fire_count, sizeof(int32_t) * e.N, cudaMemcpyDeviceToHost, e.stream));
     CK(cudaStreamSynchronize(e.stream));
-    CK(cudaMemcpy(count, e.a.fire_count, sizeof(int32_t) * e.N, cudaMemcpyDeviceToHost));
     return BSIM_OK;
 }
 

@@ -157,6 +157,14 @@ struct Engine {
     // recording
     int64_t rec_cap_alloc = 0, rec_steps_alloc = 0;
     bool rec_dirty = false;
+    // read-back of the recording: the per-cycle sort's output and scratch, sized
+    // when the recording is set up, so that reading allocates nothing
+    int32_t *rec_sorted = nullptr;
+    void *sort_tmp = nullptr;
+    size_t sort_tmp_bytes = 0;
+    // staging for state uploads and read-backs: four planes of N words (v, i_E,
+    // i_I, refrac), so the host's arrays move with one copy each, no host repacking
+    float *stage = nullptr;
     // population statistics (device arrays in a: pop_size, pop_indeg, pop_outdeg)
     bool pop_info_ready = false;
     // tiled copy, host side: synapses and work units per tile (planning the parts)

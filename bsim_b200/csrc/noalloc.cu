@@ -62,8 +62,7 @@ namespace {
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
-unsigned char *g_scratch_ptr[kMaxDevices];  // device address of g_noalloc_scratch, per device
-int g_grid[kMaxDevices];
+int g_grid[kMaxDevices];  // launch shape per device (0: not sized yet)
 
 // Errors are reported through bsim_last_error(), like every other entry point.
 int noalloc_fail(int code, const char *msg, cudaError_t st = cudaSuccess)
@@ -76,34 +75,56 @@ int noalloc_fail(int code, const char *msg, cudaError_t st = cudaSuccess)
     return record_error(code, m);
 }
 
-// Once per device, with that device current: the array's device address and
-// the launch shape. Runs inside the first call on a device.
+// The array's device address, looked up on every call with the caller's device
+// current (the lookup allocates nothing and stays right across a device reset),
+// and the launch shape, sized once per device.
 int setup_device(int dev, unsigned char **scratch, int *grid)
 {
+    void *p = nullptr;
+    cudaError_t st = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (st != cudaSuccess) return noalloc_fail(BSIM_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch)", st);
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
-        void *p = nullptr;
-        cudaError_t st = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (st != cudaSuccess) return noalloc_fail(BSIM_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch)", st);
+    if (!g_grid[dev]) {
         int sms = 0, bps = 0;
         st = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (st != cudaSuccess) return noalloc_fail(BSIM_ERR_CUDA, "cudaDeviceGetAttribute", st);
         st = step_occupancy(512, BSIM_ACC_EXACT, &bps);
         if (st != cudaSuccess) return noalloc_fail(BSIM_ERR_CUDA, "cudaOccupancyMaxActiveBlocksPerMultiprocessor", st);
         g_grid[dev] = sms * (bps > 0 ? bps : 1);
-        g_scratch_ptr[dev] = static_cast<unsigned char *>(p);
     }
-    *scratch = g_scratch_ptr[dev];
+    *scratch = static_cast<unsigned char *>(p);
     *grid = g_grid[dev];
     return BSIM_OK;
+}
+
+__device__ __forceinline__ void check_fail(int32_t *err, int code) { atomicCAS(err, 0, code); }
+
+// The check pass over the caller's arrays (within the sizes the caller gives):
+// row offsets from 0 to n_syn and ascending, targets inside the network, class
+// indices inside the table, every class of the LIF kind. Any failure raises the
+// error flag, after which the step launches return at once.
+__global__ void noalloc_check_kernel(StepArgs a, int32_t n_classes, int64_t n_syn)
+{
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t rows = a.N * a.D;
+    if (tid == 0 && (a.row_off[0] != 0 || a.row_off[rows] != n_syn)) check_fail(a.err, BSIM_DEVERR_ROWS_END);
+    for (int64_t i = tid; i < rows; i += stride)
+        if (a.row_off[i + 1] < a.row_off[i]) check_fail(a.err, BSIM_DEVERR_ROW);
+    for (int64_t k = tid; k < n_syn; k += stride)
+        if ((int64_t)a.syn[k].x >= a.N) check_fail(a.err, BSIM_DEVERR_TARGET);
+    for (int64_t j = tid; j < a.N; j += stride)
+        if ((int32_t)a.cls[j] >= n_classes) check_fail(a.err, BSIM_DEVERR_CLASS);
+    for (int64_t c = tid; c < n_classes; c += stride)
+        if (a.ctab[c].kind != BSIM_NEURON_LIF) check_fail(a.err, BSIM_DEVERR_CLASS);
 }
 
 }  // namespace
 
 extern "C" int bsim_run_noalloc(int64_t n, int32_t max_delay, void *state_dev, const float *vtmp_dev,
-                                const uint16_t *cls_dev, const bsim_class_params *ctab_dev,
-                                const int64_t *row_off_dev, const uint32_t *syn_dev, int32_t *fire_count_dev,
-                                int64_t steps, void *stream)
+                                const uint16_t *cls_dev, const bsim_class_params *ctab_dev, int32_t n_classes,
+                                const int64_t *row_off_dev, const uint32_t *syn_dev, int64_t n_synapses,
+                                int32_t *fire_count_dev, int64_t steps, void *stream)
 {
     if (n < 1 || n > kMaxN)
         return noalloc_fail(BSIM_ERR_LIMIT, "bsim_run_noalloc: n_neurons must be 1..BSIM_NOALLOC_MAX_NEURONS (32768)");
@@ -111,6 +132,8 @@ extern "C" int bsim_run_noalloc(int64_t n, int32_t max_delay, void *state_dev, c
         return noalloc_fail(BSIM_ERR_LIMIT, "bsim_run_noalloc: max_delay must be 1..BSIM_NOALLOC_MAX_DELAY (16)");
     if (!state_dev || !vtmp_dev || !cls_dev || !ctab_dev || !row_off_dev || !syn_dev || !fire_count_dev || steps < 0)
         return noalloc_fail(BSIM_ERR_ARG, "bsim_run_noalloc: null pointer or negative step count");
+    if (n_classes < 1 || n_classes > BSIM_MAX_CLASSES || n_synapses < 0)
+        return noalloc_fail(BSIM_ERR_ARG, "bsim_run_noalloc: n_classes must be 1..65535, n_synapses >= 0");
     if ((reinterpret_cast<uintptr_t>(state_dev) & 15) || (reinterpret_cast<uintptr_t>(syn_dev) & 15))
         return noalloc_fail(BSIM_ERR_ARG, "bsim_run_noalloc: state and synapse arrays must be 16-byte aligned");
     int dev = 0;
@@ -160,9 +183,34 @@ extern "C" int bsim_run_noalloc(int64_t n, int32_t max_delay, void *state_dev, c
         (st = cudaMemsetAsync(a.bitmap, 0, (size_t)a.R * a.W * sizeof(uint32_t), s)) != cudaSuccess ||
         (st = cudaMemsetAsync(ctr, 0, 4 * sizeof(unsigned long long), s)) != cudaSuccess)
         return noalloc_fail(BSIM_ERR_CUDA, "bsim_run_noalloc: clearing the scratch array", st);
+    noalloc_check_kernel<<<grid, 512, 0, s>>>(a, n_classes, n_synapses);
+    if ((st = cudaGetLastError()) != cudaSuccess) return noalloc_fail(BSIM_ERR_CUDA, "bsim_run_noalloc: check", st);
     for (int64_t k = 0; k < steps; k++) {
         st = launch_step_exact(a, grid, 512, s);
         if (st != cudaSuccess) return noalloc_fail(BSIM_ERR_CUDA, "bsim_run_noalloc: launch", st);
+    }
+    return BSIM_OK;
+}
+
+extern "C" int bsim_noalloc_status(void *stream, int32_t *device_error)
+{
+    if (!device_error) return noalloc_fail(BSIM_ERR_ARG, "bsim_noalloc_status: null output");
+    void *p = nullptr;
+    cudaError_t st = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (st != cudaSuccess) return noalloc_fail(BSIM_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch)", st);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int32_t err = 0;
+    if ((st = cudaMemcpyAsync(&err, static_cast<unsigned char *>(p) + kCtrOff + 3 * sizeof(unsigned long long),
+                              sizeof(int32_t), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (st = cudaStreamSynchronize(s)) != cudaSuccess)
+        return noalloc_fail(BSIM_ERR_CUDA, "bsim_noalloc_status", st);
+    *device_error = err;
+    if (err) {
+        static const char *names[] = {"", "row offsets not ascending", "synapse target outside the network",
+                                      "class index or kind out of range", "row offsets do not span 0..n_synapses"};
+        std::string m = "bsim_run_noalloc: device error flag " + std::to_string(err);
+        if (err > 0 && err <= 4) m += std::string(" (") + names[err] + ")";
+        return record_error(BSIM_ERR_DEVICE, m);
     }
     return BSIM_OK;
 }

@@ -37,6 +37,11 @@ static __device__ __forceinline__ void red_add_u64(unsigned long long *p, unsign
     asm volatile("red.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+// Device error flag: the first error code raised stays (BSIM_DEVERR_*). Every
+// later launch on the same flag returns at once, so the host reads the code
+// (BSIM_ERR_DEVICE) and no further cycle runs on inconsistent data.
+static __device__ __forceinline__ void raise_error(const StepArgs &a, int code) { atomicCAS(a.err, 0, code); }
+
 // ---------------------------------------------------------------------------
 // Input-drive neurons (drive.h): Constant_spikes per update_constant_neuron
 // (src/neuron/constant/constant.cu:18-22), Poisson_spikes per update_poisson_neuron
@@ -183,8 +188,13 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
 // rows; 16-byte streaming loads of two packed {target, weight} entries per
 // lane; exact int64 red.add into the target's E or I accumulator.
 // ---------------------------------------------------------------------------
-static __device__ __forceinline__ void push_one(unsigned long long *acc, uint32_t tgt, uint32_t wbits, float sc)
+static __device__ __forceinline__ void push_one(const StepArgs &a, unsigned long long *acc, uint32_t tgt,
+                                                uint32_t wbits, float sc)
 {
+    if ((int64_t)tgt >= a.N) {  // a target outside the network: flag it, touch nothing
+        raise_error(a, BSIM_DEVERR_TARGET);
+        return;
+    }
     const float w = __int_as_float(wbits);
     const long long q = __float2ll_rn(__fmul_rn(w, sc));
     red_add_u64(acc + 2 * (int64_t)tgt + (w >= 0.0f ? 0 : 1), (unsigned long long)q);
@@ -258,6 +268,10 @@ static __device__ __forceinline__ unsigned long long push_phase(const StepArgs &
             const int32_t s = a.ring[(int64_t)slot * a.cap + (item - s_cum[d - 1])];
             r0 = a.row_off[(int64_t)s * D + d - 1];
             r1 = a.row_off[(int64_t)s * D + d];
+            if (r1 < r0) {  // row offsets not ascending: flag it, skip the row
+                raise_error(a, BSIM_DEVERR_ROW);
+                r1 = r0;
+            }
             sc = __ldg(&a.ctab[a.cls[s]].scale_up);
             ev += (unsigned long long)(r1 - r0);
         }
@@ -292,7 +306,7 @@ static __device__ __forceinline__ unsigned long long push_phase(const StepArgs &
             const float sk = __shfl_sync(0xffffffffu, sc, k & (PUSH_CHUNK - 1));
             if (k < PUSH_CHUNK && ((want_head && hk) || (!want_head && tk))) {
                 const uint2 x = ld_stream8(a.syn + (want_head ? rk0 : rk1 - 1));
-                push_one(acc, x.x, x.y, sk);
+                push_one(a, acc, x.x, x.y, sk);
             }
         }
         // the pairs of all segments as one flat range, four loads in flight per lane
@@ -313,8 +327,8 @@ static __device__ __forceinline__ unsigned long long push_phase(const StepArgs &
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 if (ok[u]) {
-                    push_one(acc, x[u].x, x[u].y, xs[u]);
-                    push_one(acc, x[u].z, x[u].w, xs[u]);
+                    push_one(a, acc, x[u].x, x[u].y, xs[u]);
+                    push_one(a, acc, x[u].z, x[u].w, xs[u]);
                 }
             }
         }
@@ -767,6 +781,8 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const __grid
     __shared__ int s_last;
     // tiled delivery: [4][tile] u32 limb counters (one sign), then per-warp segment lists
     extern __shared__ __align__(16) unsigned long long s_dyn[];
+    // a raised error flag stops every later cycle (block-uniform test)
+    if (__syncthreads_or(threadIdx.x == 0 && *reinterpret_cast<volatile int32_t *>(a.err) != 0)) return;
     const unsigned long long t = *reinterpret_cast<volatile unsigned long long *>(a.step_ctr);
     const int p = (int)(t & 1ull);
     const int cur = (int)(t % (unsigned long long)a.R);

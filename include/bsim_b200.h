@@ -31,6 +31,15 @@ extern "C" {
 #define BSIM_ERR_STATE (-6)    /* call not valid in the engine's current state */
 #define BSIM_ERR_LIMIT (-7)    /* network exceeds a documented engine limit */
 
+/* Codes of the device error flag (BSIM_ERR_DEVICE; the message of bsim_last_error names
+ * the code). The first code raised is kept; every later cycle of the engine (or of the
+ * allocation-free call) returns at once, so no cycle runs on inconsistent data. */
+#define BSIM_DEVERR_ROW 1      /* a push row ends before it starts (row offsets not ascending) */
+#define BSIM_DEVERR_TARGET 2   /* a synapse target outside the network */
+#define BSIM_DEVERR_CLASS 3    /* a class index beyond the class table, or a class of a kind
+                                  the entry point does not take */
+#define BSIM_DEVERR_ROWS_END 4 /* row offsets do not start at 0 or do not end at the synapse count */
+
 #define BSIM_MAX_DELAY 1024    /* delays are 1..BSIM_MAX_DELAY steps */
 #define BSIM_MAX_CLASSES 65535 /* distinct folded LIF parameter tuples per engine */
 
@@ -313,8 +322,9 @@ const char *bsim_last_error(void);
  * max_delay <= BSIM_NOALLOC_MAX_DELAY; larger sizes return BSIM_ERR_LIMIT. No
  * cudaMalloc, cudaFree or other allocating routine is called.
  *
- * The first call on a device looks the array up (cudaGetSymbolAddress) with
- * that device current; make that first call before any stream capture.
+ * Every call looks the array's device address up (cudaGetSymbolAddress) with the
+ * caller's current device, so a device reset between calls is harmless; the first
+ * call on a device also sizes the launch, so make it before any stream capture.
  * All calls on a device share the array and each call clears it first: calls
  * whose GPU work overlaps (other streams, unordered threads) race on it.
  *
@@ -323,12 +333,19 @@ const char *bsim_last_error(void);
  * spikes in flight, and returns once the work is enqueued.
  *   state_dev      [n] float4 {v, i_E, i_I, refrac_step bit pattern}, in/out, 16-byte aligned
  *   vtmp_dev       [n] (i_offset * rm + v_rest) * (1 - Cm), as LIFENeuron::reset folds it
- *   cls_dev        [n] class of each neuron
- *   ctab_dev       [classes] folded constants, scale_up = 2^qexp, scale_down = 2^-qexp
- *   row_off_dev    [n * max_delay + 1] rows by (source, delay - 1), delay-minor
- *   syn_dev        [2 * entries] {target id, weight bit pattern} per entry, 16-byte aligned
+ *   cls_dev        [n] class of each neuron, < n_classes
+ *   ctab_dev       [n_classes] folded constants, scale_up = 2^qexp, scale_down = 2^-qexp,
+ *                  kind = BSIM_NEURON_LIF
+ *   row_off_dev    [n * max_delay + 1] rows by (source, delay - 1), delay-minor, ascending,
+ *                  from 0 to n_synapses
+ *   syn_dev        [2 * n_synapses] {target id < n, weight bit pattern} per entry, 16-byte aligned
  *   fire_count_dev [n] incremented by each neuron's spikes
- */
+ * Before the first cycle a check pass on the GPU reads these arrays (within the sizes
+ * given) and raises the device error flag (BSIM_DEVERR_*) on a class index, kind, row
+ * offset or target out of range; the cycles then do nothing. bsim_noalloc_status reads
+ * the flag. Not checked: the numeric values of the state and of the folded constants,
+ * and that each array really holds the number of elements stated; the arrays must not
+ * change while the call's work runs. */
 #define BSIM_NOALLOC_MAX_NEURONS 32768
 #define BSIM_NOALLOC_MAX_DELAY 16
 
@@ -343,8 +360,16 @@ typedef struct bsim_class_params {
 } bsim_class_params;
 
 int bsim_run_noalloc(int64_t n, int32_t max_delay, void *state_dev, const float *vtmp_dev, const uint16_t *cls_dev,
-                     const bsim_class_params *ctab_dev, const int64_t *row_off_dev, const uint32_t *syn_dev,
-                     int32_t *fire_count_dev, int64_t steps, void *stream);
+                     const bsim_class_params *ctab_dev, int32_t n_classes, const int64_t *row_off_dev,
+                     const uint32_t *syn_dev, int64_t n_synapses, int32_t *fire_count_dev, int64_t steps,
+                     void *stream);
+
+/* Waits for `stream` and copies the device error flag of the most recent
+ * bsim_run_noalloc call on the current device into *device_error (a host int;
+ * 0 = no error, else a BSIM_DEVERR_* code). Returns BSIM_OK when the flag is 0,
+ * BSIM_ERR_DEVICE when it is set. Allocates nothing. The allocation-free call's
+ * companion: it has no counterpart in the reference either. */
+int bsim_noalloc_status(void *stream, int32_t *device_error);
 
 #ifdef __cplusplus
 }

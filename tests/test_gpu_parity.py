@@ -253,3 +253,94 @@ def test_square_wave_drive_vs_oracle():
     lo_rate = sum(len(r) for r in fx["raster"][:60]) / 60
     hi_rate = sum(len(r) for r in fx["raster"][60:120]) / 60
     assert hi_rate > 3 * lo_rate
+
+
+# ---------------------------------------------------------------------------
+# Tiled and AUTO delivery (the benchmark's default modes) against the oracle at
+# the shapes the benchmark runs: scaled replicas of the 1e6-neuron (100
+# populations, delays 1-6), dense (50 populations, delays 1-50) and
+# predictor-scheduled (200 populations, delays 1-20, square-wave drive)
+# configurations, with the automatic tile size (many parts per tile, so most
+# blocks help), tiles straddling populations with ~3 parts each, and one tile
+# for the whole network (every block but one helps). Reference semantics:
+# update_dense_static_hit, src/synapse/static/static.cu:59-96.
+# ---------------------------------------------------------------------------
+_FIXED = {}
+
+
+def replica(name):
+    if name == "plain":
+        return W.scaled(W.plain_1m(1)[0][0], 200)
+    if name == "dense":
+        return W.scaled(W.dense_1m(1)[0][0], 400)
+    if name == "square":
+        return W.scaled(W.predicted_2m(1)[0][0], 100)
+    raise KeyError(name)
+
+
+def fixed_reference(name, steps, qexp):
+    """The fixed-point oracle's run of a replica (cached per test session)."""
+    key = (name, steps, qexp)
+    if key not in _FIXED:
+        spec = replica(name)
+        g = B.gen_host(spec)
+        kw = {}
+        if spec.drive_half_period > 0:
+            hi = g["params"].copy()
+            hi[:, 9] = (g["params"][:, 9] * np.float32(spec.drive_scale)).astype(np.float32)
+            kw = dict(params_alt=hi, half_period=int(spec.drive_half_period))
+        _FIXED[key] = (g, oracle.run(g["params"], g["src"], g["dst"], g["weight"], g["delay_steps"], DT, steps,
+                                     record_steps=steps, rec_ids=np.arange(g["params"].shape[0]),
+                                     acc_mode=oracle.ACC_FIXED, qexp=qexp, **kw))
+    return _FIXED[key]
+
+
+def check_vs_fixed(eng, name, steps):
+    raster, vs = run_checkpoints(eng, steps, steps)
+    g, fx = fixed_reference(name, steps, int(eng.qexp()[0]))
+    assert sum(len(r) for r in raster) > 0
+    assert same_raster(raster, fx["raster"]) is None
+    assert np.array_equal(vs[-1], fx["v_trace"][-1])
+    assert np.array_equal(eng.fire_count(), fx["fire_count"])
+    assert eng.info().events_total == fx["events_per_step"].sum()
+
+
+@pytest.mark.parametrize("name,opts", [
+    ("plain", dict()),
+    ("plain", dict(tile_size=150)),
+    ("plain", dict(tile_size=20000)),
+    ("dense", dict()),
+    ("square", dict()),
+])
+def test_tiled_delivery_vs_oracle_at_bench_shapes(name, opts):
+    eng = B.Engine.generated(replica(name), DT, opts=B.options(delivery=B.DELIVERY_TILE, **opts))
+    check_vs_fixed(eng, name, 1000)
+
+
+def test_auto_delivery_vs_oracle_switching_modes():
+    """AUTO delivery under the firing predictor, with cost models whose crossover
+    sits inside the network's range of activity, so that cycles go both ways:
+    still bit-identical to the oracle."""
+    spec = replica("plain")
+    eng = B.Engine.generated(spec, DT, opts=B.options(delivery=B.DELIVERY_AUTO))
+    eng.enable_pop_stats(64)
+    g, fx = fixed_reference("plain", 1000, int(eng.qexp()[0]))
+    work = np.median(fx["events_per_step"][100:])
+    eng.set_predictor(B.mlp_init(5), tolerance=0.25, cost_push=[0.0, 1.0], cost_tile=[float(work), 0.0])
+    check_vs_fixed(eng, "plain", 1000)
+    st = eng.predictor_stats()
+    assert 0 < st.tile_cycles < st.cycles
+
+
+def test_tiled_delivery_rates_over_a_full_second():
+    """10,000 cycles (1 s) of the 1e6-neuron configuration's replica with tiled
+    delivery: per-population rates within 1 % of the reference order."""
+    spec = replica("plain")
+    g = B.gen_host(spec)
+    eng = B.Engine.generated(spec, DT, opts=B.options(delivery=B.DELIVERY_TILE))
+    eng.run(10000)
+    sq = oracle_run(g, 10000, oracle.ACC_SEQUENTIAL, rec_ids=np.zeros(0, np.int32))
+    ra = eng.fire_count().reshape(spec.n_pop, -1).sum(1).astype(np.float64)
+    rb = sq["fire_count"].reshape(spec.n_pop, -1).sum(1).astype(np.float64)
+    assert rb.sum() > 0
+    assert np.all(np.abs(ra - rb) <= 0.01 * np.maximum(rb, 100))
