@@ -163,11 +163,12 @@ def reduce_over_ranks(dist, maxes, sums, device="cpu"):
 # CPU baselines (oracle/_ref: the reference's own simulator, else the oracle port)
 # ---------------------------------------------------------------------------
 def replica_net(spec, pop_size):
-    """Scaled-down replica of a generated workload, in the reference API's terms."""
-    import bsim_b200 as B
+    """Scaled-down replica of a generated workload, in the reference API's terms. The
+    generator is the oracle library's copy, so the CPU arms never load the engine."""
     from bsim_b200 import workloads as W
+    from oracle import oracle
     rs = W.scaled(spec, pop_size)
-    g = B.gen_host(rs)
+    g = oracle.gen_host(rs)
     dt = np.float32(DT)
     net = dict(params=g["params"].astype(np.float64), pop_size=np.full(rs.n_pop, rs.pop_size, np.int64),
                pop_tau=np.tile([rs.tau_syn_E, rs.tau_syn_I], (rs.n_pop, 1)).astype(np.float64),

@@ -823,11 +823,6 @@ struct GenInst {
     int32_t out_off;     // into the outgoing table: [P][3] (count, projection ids)
 };
 
-struct GenProj {
-    int32_t src_pop, dst_pop;
-    uint64_t pseed;
-};
-
 struct GenDev {
     const GenInst *inst;
     int32_t n_inst;
@@ -1052,55 +1047,12 @@ __global__ void gen_tile_kernel(const TileSeg *segs, int n_segs, int64_t n_pairs
     }
 }
 
-// Remote projection choice of one generated network (host side, shared by
-// the host generator and the device builder).
-struct GenPlan {
-    std::vector<GenProj> proj;              // creation order
-    std::vector<std::vector<int>> in, out;  // per population: projection ids in creation order
-};
-
-static GenPlan gen_plan(const bsim_gen_spec &g)
-{
-    GenPlan pl;
-    const int P = g.n_pop;
-    pl.in.assign(P, {});
-    pl.out.assign(P, {});
-    for (int k = 0; k + 1 < P; k++) pl.proj.push_back({k, k + 1, proj_seed(g.seed, k)});
-    if (P >= 2) {
-        int m = (int)(g.remote_frac * (float)P + 0.5f);
-        m = std::min(m, P);
-        std::vector<std::pair<uint64_t, int>> keys;
-        for (int k = 0; k < P; k++) keys.push_back({hash3(g.seed ^ SALT_REMOTE_SEL, (uint64_t)k, 0), k});
-        std::sort(keys.begin(), keys.end());
-        std::vector<int> sel;
-        for (int r = 0; r < m; r++) sel.push_back(keys[r].second);
-        std::sort(sel.begin(), sel.end());
-        for (int k : sel) {
-            uint64_t h = hash3(g.seed ^ SALT_REMOTE_TGT, (uint64_t)k, 0);
-            int tgt = (int)((k + 1 + (int64_t)(h % (uint64_t)(P - 1))) % P);
-            int id = (int)pl.proj.size();
-            pl.proj.push_back({k, tgt, proj_seed(g.seed, id)});
-        }
-    }
-    for (int id = 0; id < (int)pl.proj.size(); id++) {
-        pl.out[pl.proj[id].src_pop].push_back(id);
-        pl.in[pl.proj[id].dst_pop].push_back(id);
-    }
-    return pl;
-}
-
 static int check_spec(const bsim_gen_spec &g)
 {
     if (g.n_pop < 1 || g.pop_size < 1 || g.max_delay < 1 || g.max_delay > GEN_MAX_DELAY ||
         (int64_t)g.n_pop * g.pop_size > (int64_t)INT32_MAX / 2 || !(g.p_conn >= 0) || g.p_conn > 1)
         return fail(BSIM_ERR_ARG, "bsim_gen_spec: invalid sizes (max_delay 1..64, p_conn in [0,1])");
     return BSIM_OK;
-}
-
-static void spec_params(const bsim_gen_spec &g, float ioff, float vinit, float *p)
-{
-    p[0] = vinit; p[1] = g.v_rest; p[2] = g.v_reset; p[3] = g.cm; p[4] = g.tau_m;
-    p[5] = g.tau_refrac; p[6] = g.tau_syn_E; p[7] = g.tau_syn_I; p[8] = g.v_thresh; p[9] = ioff;
 }
 
 static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, const bsim_options *opt, Engine **out)
@@ -1389,41 +1341,12 @@ static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, co
     return BSIM_OK;
 }
 
-// Host generator: the same draws, emitted in global creation order.
+// Host generator: the same draws, emitted in global creation order (netgen.h).
 static int gen_host(const bsim_gen_spec &g, float *params, int32_t *pop, int32_t *src, int32_t *dst, float *w,
                     int32_t *d, int64_t *n_out, int64_t *s_out)
 {
     TRY(check_spec(g));
-    GenPlan pl = gen_plan(g);
-    const int64_t n = (int64_t)g.n_pop * g.pop_size;
-    if (params || pop) {
-        for (int64_t i = 0; i < n; i++) {
-            float ioff, vinit;
-            draw_neuron(g.seed, (uint64_t)i, g, &ioff, &vinit);
-            if (params) spec_params(g, ioff, vinit, params + 10 * i);
-            if (pop) pop[i] = (int32_t)(i / g.pop_size);
-        }
-    }
-    const uint32_t p24 = prob24(g.p_conn), exc24 = prob24(g.exc_frac);
-    const float w_exc = g.w_max, w_inh = g.inh_scale * g.w_max;
-    int64_t s = 0;
-    for (const GenProj &pr : pl.proj) {
-        for (int64_t i = 0; i < g.pop_size; i++) {
-            for (int64_t j = 0; j < g.pop_size; j++) {
-                SynDraw sd;
-                if (!draw_pair(pr.pseed, (uint64_t)i, (uint64_t)j, p24, exc24, w_exc, w_inh, g.max_delay, &sd)) continue;
-                if (src) {
-                    src[s] = (int32_t)(pr.src_pop * (int64_t)g.pop_size + i);
-                    dst[s] = (int32_t)(pr.dst_pop * (int64_t)g.pop_size + j);
-                    w[s] = sd.w;
-                    d[s] = sd.d;
-                }
-                s++;
-            }
-        }
-    }
-    if (n_out) *n_out = n;
-    if (s_out) *s_out = s;
+    netgen_host(g, params, pop, src, dst, w, d, n_out, s_out);
     return BSIM_OK;
 }
 

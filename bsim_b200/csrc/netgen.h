@@ -18,6 +18,10 @@
 #pragma once
 #include <stdint.h>
 
+#include <algorithm>
+#include <utility>
+#include <vector>
+
 #include "../../include/bsim_b200.h"
 
 #if defined(__CUDACC__)
@@ -123,5 +127,94 @@ BSIM_HD void draw_neuron(uint64_t seed, uint64_t gid_local, const bsim_gen_spec 
 }
 
 BSIM_HD uint64_t proj_seed(uint64_t seed, int32_t proj) { return hash3(seed ^ SALT_PROJ, (uint64_t)proj, 7); }
+
+// ---------------------------------------------------------------------------
+// Host side (shared by the host generator, the device builder's planning and
+// the CPU oracle's copy of the generator).
+// ---------------------------------------------------------------------------
+struct GenProj {
+    int32_t src_pop, dst_pop;
+    uint64_t pseed;
+};
+
+// Remote projection choice of one generated network.
+struct GenPlan {
+    std::vector<GenProj> proj;              // creation order
+    std::vector<std::vector<int>> in, out;  // per population: projection ids in creation order
+};
+
+inline GenPlan gen_plan(const bsim_gen_spec &g)
+{
+    GenPlan pl;
+    const int P = g.n_pop;
+    pl.in.assign(P, {});
+    pl.out.assign(P, {});
+    for (int k = 0; k + 1 < P; k++) pl.proj.push_back({k, k + 1, proj_seed(g.seed, k)});
+    if (P >= 2) {
+        int m = (int)(g.remote_frac * (float)P + 0.5f);
+        m = std::min(m, P);
+        std::vector<std::pair<uint64_t, int>> keys;
+        for (int k = 0; k < P; k++) keys.push_back({hash3(g.seed ^ SALT_REMOTE_SEL, (uint64_t)k, 0), k});
+        std::sort(keys.begin(), keys.end());
+        std::vector<int> sel;
+        for (int r = 0; r < m; r++) sel.push_back(keys[r].second);
+        std::sort(sel.begin(), sel.end());
+        for (int k : sel) {
+            uint64_t h = hash3(g.seed ^ SALT_REMOTE_TGT, (uint64_t)k, 0);
+            int tgt = (int)((k + 1 + (int64_t)(h % (uint64_t)(P - 1))) % P);
+            int id = (int)pl.proj.size();
+            pl.proj.push_back({k, tgt, proj_seed(g.seed, id)});
+        }
+    }
+    for (int id = 0; id < (int)pl.proj.size(); id++) {
+        pl.out[pl.proj[id].src_pop].push_back(id);
+        pl.in[pl.proj[id].dst_pop].push_back(id);
+    }
+    return pl;
+}
+
+// LIFENeuron constructor arguments of one generated neuron.
+inline void spec_params(const bsim_gen_spec &g, float ioff, float vinit, float *p)
+{
+    p[0] = vinit; p[1] = g.v_rest; p[2] = g.v_reset; p[3] = g.cm; p[4] = g.tau_m;
+    p[5] = g.tau_refrac; p[6] = g.tau_syn_E; p[7] = g.tau_syn_I; p[8] = g.v_thresh; p[9] = ioff;
+}
+
+// The whole network as flat arrays in global creation order (any output may be
+// NULL; with src NULL only the sizes are produced). The spec must be valid.
+inline void netgen_host(const bsim_gen_spec &g, float *params, int32_t *pop, int32_t *src, int32_t *dst, float *w,
+                        int32_t *d, int64_t *n_out, int64_t *s_out)
+{
+    GenPlan pl = gen_plan(g);
+    const int64_t n = (int64_t)g.n_pop * g.pop_size;
+    if (params || pop) {
+        for (int64_t i = 0; i < n; i++) {
+            float ioff, vinit;
+            draw_neuron(g.seed, (uint64_t)i, g, &ioff, &vinit);
+            if (params) spec_params(g, ioff, vinit, params + 10 * i);
+            if (pop) pop[i] = (int32_t)(i / g.pop_size);
+        }
+    }
+    const uint32_t p24 = prob24(g.p_conn), exc24 = prob24(g.exc_frac);
+    const float w_exc = g.w_max, w_inh = g.inh_scale * g.w_max;
+    int64_t s = 0;
+    for (const GenProj &pr : pl.proj) {
+        for (int64_t i = 0; i < g.pop_size; i++) {
+            for (int64_t j = 0; j < g.pop_size; j++) {
+                SynDraw sd;
+                if (!draw_pair(pr.pseed, (uint64_t)i, (uint64_t)j, p24, exc24, w_exc, w_inh, g.max_delay, &sd)) continue;
+                if (src) {
+                    src[s] = (int32_t)(pr.src_pop * (int64_t)g.pop_size + i);
+                    dst[s] = (int32_t)(pr.dst_pop * (int64_t)g.pop_size + j);
+                    w[s] = sd.w;
+                    d[s] = sd.d;
+                }
+                s++;
+            }
+        }
+    }
+    if (n_out) *n_out = n;
+    if (s_out) *s_out = s;
+}
 
 }  // namespace bsim

@@ -27,8 +27,9 @@ def build():
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
 
 
-def build_ref(ref_root="/root/reference"):
-    """Compile the reference's own simulator driver into oracle/_ref/ when its sources exist."""
+def build_ref(ref_root):
+    """Compile the reference's own simulator driver into oracle/_ref/ from the reference's
+    source root `ref_root`, when its sources exist there."""
     if not os.path.isdir(os.path.join(ref_root, "src")):
         return False
     subprocess.run(["make", "-s", "-C", HERE, "ref", "REF=" + ref_root], check=True)
@@ -55,6 +56,10 @@ def lib():
             f.restype = ctypes.c_int
         L.oracle_poisson_draws.argtypes = [ctypes.c_uint64, ctypes.c_float, i64, P]
         L.oracle_poisson_draws.restype = ctypes.c_int
+        L.oracle_gen_count.argtypes = [P, P, P]
+        L.oracle_gen_count.restype = ctypes.c_int
+        L.oracle_gen_host.argtypes = [P, P, P, P, P, P, P]
+        L.oracle_gen_host.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -219,3 +224,24 @@ def run_reference(net_path, out_path, precision="f32", record=True, n=None, n_re
     offs = np.concatenate([[0], np.cumsum(counts)])
     raster = [ids[offs[t]:offs[t + 1]] for t in range(nrs)]
     return dict(raster=raster, v_trace=v, fire_count=fire_count, last_input=last, seconds=secs)
+
+
+def gen_host(spec):
+    """The seeded workload generator (the engine's own netgen.h, compiled into the oracle
+    library): (params[n,10] f32, pop[n], src, dst, weight f32, delay_steps) in creation
+    order, for a bsim_gen_spec, without loading the engine library."""
+    L = lib()
+    n, s = ctypes.c_int64(), ctypes.c_int64()
+    if L.oracle_gen_count(ctypes.byref(spec), ctypes.byref(n), ctypes.byref(s)) != 0:
+        raise ValueError("invalid generator spec")
+    n, s = n.value, s.value
+    params = np.zeros((n, 10), np.float32)
+    pop = np.zeros(n, np.int32)
+    src = np.zeros(s, np.int32)
+    dst = np.zeros(s, np.int32)
+    w = np.zeros(s, np.float32)
+    d = np.zeros(s, np.int32)
+    ptr = lambda a: ctypes.c_void_p(a.ctypes.data)
+    if L.oracle_gen_host(ctypes.byref(spec), ptr(params), ptr(pop), ptr(src), ptr(dst), ptr(w), ptr(d)) != 0:
+        raise ValueError("invalid generator spec")
+    return dict(params=params, pop=pop, src=src, dst=dst, weight=w, delay_steps=d)

@@ -5,14 +5,16 @@ simulation cycle, dt = 0.1 ms) of 30 values printed with "%.10lf \\t" (the v of 
 3x10 LIF_brian nets built in test/gpu/lif_unit{1..4}_test.cpp). The traces are kept
 verbatim as float64 so that tests can compare at the printed precision.
 
-Run:  python tests/golden/make_golden.py [/path/to/BSim]
+Run:  python tests/golden/make_golden.py /path/to/BSim
 """
 import os
 import sys
 
 import numpy as np
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    raise SystemExit("usage: make_golden.py <root of the BSim project>")
+ref = sys.argv[1]
 out = {}
 for k in (1, 2, 3, 4):
     path = os.path.join(ref, "test", "lif_unit%d_test_v.std" % k)

@@ -146,3 +146,18 @@ def test_oracle_bit_exact_vs_reference_generated_net(shape):
         assert np.array_equal(a, b)
     assert np.array_equal(ref["v_trace"], r["v_trace"].astype(np.float64))
     assert np.array_equal(ref["fire_count"], r["fire_count"])
+
+
+def test_oracle_generator_equals_engine_generator():
+    """The oracle library's copy of the workload generator (used by the CPU
+    baselines, which never load the engine) gives the engine's networks bit for bit."""
+    import bsim_b200 as B
+    from bsim_b200 import workloads as W
+    for sp in (W.cuba(10, 300, 100, 6, seed=3), W.scaled(W.dense_1m(1)[0][0], 60),
+               W.scaled(W.predicted_2m(1)[0][0], 40)):
+        a, b = B.gen_host(sp), oracle.gen_host(sp)
+        assert len(a["src"]) > 0
+        for k in a:
+            assert a[k].dtype == b[k].dtype and np.array_equal(a[k].view(np.uint32) if a[k].dtype == np.float32
+                                                               else a[k], b[k].view(np.uint32)
+                                                               if b[k].dtype == np.float32 else b[k])
