@@ -40,7 +40,7 @@ class Options(ctypes.Structure):
                 ("build_pull", ctypes.c_int32), ("graph_steps", ctypes.c_int32),
                 ("block_threads", ctypes.c_int32), ("grid_blocks", ctypes.c_int32),
                 ("build_tiles", ctypes.c_int32), ("tile_size", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 7)]
+                ("lif_blocks", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6)]
 
 
 class GenSpec(ctypes.Structure):
@@ -131,6 +131,8 @@ def lib():
             "bsim_set_predictor": [P, P, f32, P, P],
             "bsim_predictor_stats": [P, P],
             "bsim_autotune": [P, i32, P],
+            "bsim_trace": [P, i64, i64, i64],
+            "bsim_read_trace": [P, P, P, P, P, P, P],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -304,6 +306,23 @@ class Engine:
             ids = np.empty(max(total, 1), np.int32)
         _check(lib().bsim_read_raster(self._h, _p(off), _p(ids), ids.shape[0], ctypes.byref(ns)))
         return [ids[off[k]:off[k + 1]] for k in range(ns.value)]
+
+    def trace(self, max_steps, first=0, count=None):
+        """Traces v, i_E, i_I and the consumed synaptic input (E, I) of neurons
+        [first, first + count) after each of the next max_steps cycles, on the device."""
+        if count is None:
+            count = self.info().n_neurons - first
+        _check(lib().bsim_trace(self._h, max_steps, first, count))
+        self._trace_shape = (max_steps, count)
+
+    def read_trace(self):
+        """The trace so far: dict of [n_steps, count] float32 arrays v, i_E, i_I, in_E, in_I."""
+        steps, count = self._trace_shape
+        out = {k: np.zeros((steps, count), np.float32) for k in ("v", "i_E", "i_I", "in_E", "in_I")}
+        ns = ctypes.c_int64()
+        _check(lib().bsim_read_trace(self._h, _p(out["v"]), _p(out["i_E"]), _p(out["i_I"]), _p(out["in_E"]),
+                                     _p(out["in_I"]), ctypes.byref(ns)))
+        return {k: v[:ns.value] for k, v in out.items()}
 
     def state(self):
         n = self.info().n_neurons

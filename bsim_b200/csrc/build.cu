@@ -530,6 +530,7 @@ static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
     a.delivery = (e.opt.delivery == BSIM_DELIVERY_PULL || e.opt.delivery == BSIM_DELIVERY_AUTO) ? e.opt.delivery
                                                                                                  : BSIM_DELIVERY_PUSH;
     a.deliv_sel = nullptr;
+    a.lif_blocks = e.opt.lif_blocks;
     a.rec_ids = nullptr;
     a.rec_off = nullptr;
     a.rec = nullptr;
@@ -1604,6 +1605,61 @@ int bsim_read_raster(bsim_engine *eh, int64_t *step_off, int32_t *ids, int64_t i
         CK(cudaMemcpyAsync(ids, e.rec_sorted, sizeof(int32_t) * total, cudaMemcpyDeviceToHost, e.stream));
         CK(cudaStreamSynchronize(e.stream));
     }
+    return BSIM_OK;
+}
+
+int bsim_trace(bsim_engine *eh, int64_t max_steps, int64_t first, int64_t count)
+{
+    if (!eh || max_steps < 0 || first < 0 || count < 0) return fail(BSIM_ERR_ARG, "bsim_trace: invalid arguments");
+    Engine &e = *H(eh);
+    if (first + count > e.N) return fail(BSIM_ERR_ARG, "bsim_trace: neuron range beyond the network");
+    CK(cudaSetDevice(e.device));
+    CK(cudaStreamSynchronize(e.stream));
+    bool dirty = false;
+    if (!e.a.trace_ctl) {
+        TraceCtl *tc;
+        TRY(dalloc(e, &tc, 1));
+        e.a.trace_ctl = tc;
+        dirty = true;
+    }
+    const int64_t need = 5 * max_steps * count;
+    if (need > e.trace_alloc || !e.a.trace) {
+        float *buf;
+        TRY(dalloc(e, &buf, std::max<int64_t>(need, 1)));
+        e.a.trace = buf;
+        e.trace_alloc = std::max<int64_t>(need, 1);
+        dirty = true;
+    }
+    TraceCtl ctl{e.steps_done, max_steps, first, count};
+    CK(cudaMemcpy(const_cast<TraceCtl *>(e.a.trace_ctl), &ctl, sizeof(ctl), cudaMemcpyHostToDevice));
+    if (dirty) {  // the captured graph holds the old arguments
+        if (e.graph_exec) { cudaGraphExecDestroy(e.graph_exec); e.graph_exec = nullptr; }
+        if (e.graph) { cudaGraphDestroy(e.graph); e.graph = nullptr; }
+    }
+    return BSIM_OK;
+}
+
+int bsim_read_trace(bsim_engine *eh, float *v, float *iE, float *iI, float *in_E, float *in_I, int64_t *n_steps)
+{
+    if (!eh || !n_steps) return fail(BSIM_ERR_ARG, "bsim_read_trace: invalid arguments");
+    Engine &e = *H(eh);
+    if (!e.a.trace || !e.a.trace_ctl) return fail(BSIM_ERR_STATE, "bsim_read_trace: tracing not enabled");
+    CK(cudaSetDevice(e.device));
+    TraceCtl ctl;
+    CK(cudaMemcpyAsync(&ctl, e.a.trace_ctl, sizeof(ctl), cudaMemcpyDeviceToHost, e.stream));
+    unsigned long long done = 0;
+    CK(cudaMemcpyAsync(&done, e.a.step_ctr, sizeof(done), cudaMemcpyDeviceToHost, e.stream));
+    CK(cudaStreamSynchronize(e.stream));
+    int64_t ns = (int64_t)done - ctl.t0;
+    ns = std::max<int64_t>(0, std::min<int64_t>(ns, ctl.steps));
+    *n_steps = ns;
+    float *dst[5] = {v, iE, iI, in_E, in_I};
+    const int64_t plane = ctl.steps * ctl.count;
+    for (int f = 0; f < 5; f++)
+        if (dst[f] && ns > 0)
+            CK(cudaMemcpyAsync(dst[f], e.a.trace + f * plane, sizeof(float) * ns * ctl.count, cudaMemcpyDeviceToHost,
+                               e.stream));
+    CK(cudaStreamSynchronize(e.stream));
     return BSIM_OK;
 }
 

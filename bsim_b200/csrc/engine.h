@@ -39,6 +39,16 @@ struct RecCtl {
     long long cap;
 };
 
+// State trace window: after each cycle t in [t0, t0 + steps), the neurons
+// [first, first + count) have v, i_E, i_I and the synaptic input the cycle
+// consumed (E, I) copied into the trace buffer, field-major: [5][steps][count].
+struct TraceCtl {
+    long long t0;
+    long long steps;  // 0: not tracing
+    long long first;
+    long long count;
+};
+
 // Firing-predictor statistics, accumulated on the device.
 struct PredStats {
     unsigned long long cycles, fallbacks, tile_cycles;
@@ -82,10 +92,14 @@ struct StepArgs {
     int32_t *err;                  // device error flag (0 = ok)
     const int32_t *deliv_sel;      // per-step delivery choice written by the predictor (may be NULL)
     int32_t delivery;              // BSIM_DELIVERY_PUSH / _PULL when deliv_sel is NULL
+    int32_t lif_blocks;            // blocks [0, lif_blocks) run the neuron update (grid-stride over them)
     // raster recording (control words in device memory so a captured graph stays valid)
     int32_t *rec_ids;           // [rec->cap]
     int64_t *rec_off;           // [rec->steps + 1]
     struct RecCtl *rec;         // NULL: recording never enabled
+    // state trace (the reference's LOG_DATA files g_v / g_ie / g_ii / g_input_e / g_input_i)
+    float *trace;               // [5][trace_ctl->steps][trace_ctl->count] (NULL: never enabled)
+    const struct TraceCtl *trace_ctl;
     // per-population spike counts of the last hist_len steps (predictor input)
     int32_t *pop_hist;          // [hist_len][n_pops]
     int32_t n_pops, hist_len;
@@ -157,6 +171,7 @@ struct Engine {
     // recording
     int64_t rec_cap_alloc = 0, rec_steps_alloc = 0;
     bool rec_dirty = false;
+    int64_t trace_alloc = 0;  // floats in the trace buffer
     // read-back of the recording: the per-cycle sort's output and scratch, sized
     // when the recording is set up, so that reading allocates nothing
     int32_t *rec_sorted = nullptr;

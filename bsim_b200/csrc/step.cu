@@ -84,11 +84,25 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
                                                  int *s_wcnt)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int nb = (a.lif_blocks > 0 && a.lif_blocks < (int)gridDim.x) ? a.lif_blocks : (int)gridDim.x;
+    if ((int)blockIdx.x >= nb) return;  // this block starts delivering at once
+    const int64_t stride = (int64_t)nb * blockDim.x;
     int32_t *slot_ids = a.ring + (int64_t)cur * a.cap;
     uint32_t *bm = a.bitmap + (int64_t)cur * a.W;
     int32_t *hist = a.pop_hist ? a.pop_hist + (int64_t)(t % (unsigned long long)a.hist_len) * a.n_pops : nullptr;
     const float *vtmp = (a.drive_half > 0 && ((t / (unsigned long long)a.drive_half) & 1ull)) ? a.vtmp_alt : a.vtmp;
+    // state trace of this cycle: the row, or -1
+    long long tr_k = -1, tr_first = 0, tr_count = 0, tr_steps = 0;
+    if (a.trace) {
+        const TraceCtl tc = *a.trace_ctl;
+        const long long k = (long long)t - tc.t0;
+        if (k >= 0 && k < tc.steps) {
+            tr_k = k;
+            tr_first = tc.first;
+            tr_count = tc.count;
+            tr_steps = tc.steps;
+        }
+    }
     for (int64_t bbase = (int64_t)blockIdx.x * blockDim.x; bbase < a.N; bbase += stride) {
         const int64_t base = bbase + (threadIdx.x & ~31);
         const int64_t j = base + lane;
@@ -147,6 +161,15 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
                 drive_update(a, kind, j, (int)t, c, st, fired);  // input is dropped (recv returns 0)
             }
             a.state[j] = st;
+            if (tr_k >= 0 && j >= tr_first && j < tr_first + tr_count) {
+                const int64_t plane = tr_steps * tr_count;
+                float *row = a.trace + tr_k * tr_count + (j - tr_first);
+                row[0] = st.x;
+                row[plane] = st.y;
+                row[2 * plane] = st.z;
+                row[3 * plane] = inE;
+                row[4 * plane] = inI;
+            }
             if (hist) pop = __ldg(&c->pop);
         }
         const unsigned mask = __ballot_sync(0xffffffffu, fired);

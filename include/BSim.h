@@ -496,36 +496,50 @@ public:
 
 private:
 #ifdef LOG_DATA
+    // The reference's LOG_DATA files (SingleGPUSimulator.cu:150-242): per cycle one line
+    // of fired ids (GSim.log; ascending here, in atomic order there) and one line of
+    // "%.10lf \t" values per neuron for v, i_E, i_I and the synaptic input the cycle
+    // consumed. The engine records spikes and the state trace on the device inside the
+    // step; the host reads them back once per chunk of cycles (sized to ~256 MB of
+    // buffers), not once per cycle.
     int run_logged(bsim_engine *e, int cycles, int64_t n)
     {
-        FILE *lf = fopen("GSim.log", "w+"), *vf = fopen("g_v.data", "w+");
-        FILE *ef = fopen("g_ie.data", "w+"), *jf = fopen("g_ii.data", "w+");
-        if (!lf || !vf || !ef || !jf) return -1;
-        std::vector<float> v(n), ie(n), ii(n);
-        std::vector<int64_t> off(2);
-        std::vector<int32_t> ids(n);
+        const char *names[6] = {"GSim.log", "g_v.data", "g_ie.data", "g_ii.data", "g_input_e.data",
+                                "g_input_i.data"};
+        FILE *f[6];
+        for (int k = 0; k < 6; k++) f[k] = fopen(names[k], "w+");
         int rc = BSIM_OK;
-        for (int t = 0; t < cycles && rc == BSIM_OK; t++) {
-            bsim_record(e, 1, n);
-            rc = bsim_run(e, 1);
-            int64_t ns = 0;
-            if (rc == BSIM_OK) rc = bsim_read_raster(e, off.data(), ids.data(), n, &ns);
-            if (rc == BSIM_OK) rc = bsim_read_state(e, v.data(), ie.data(), ii.data(), NULL);
-            for (int64_t k = 0; k < (ns ? off[1] : 0); k++) fprintf(lf, "%d ", ids[k]);
-            fprintf(lf, "\n");
-            for (int64_t i = 0; i < n; i++) {
-                fprintf(vf, "%.10lf \t", (double)v[i]);
-                fprintf(ef, "%.10lf \t", (double)ie[i]);
-                fprintf(jf, "%.10lf \t", (double)ii[i]);
+        for (int k = 0; k < 6; k++)
+            if (!f[k]) rc = -1;
+        const int64_t per_cycle = 4 * (6 * n + 2);
+        const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(cycles, (256LL << 20) / per_cycle));
+        std::vector<float> tr(5 * chunk * n);
+        std::vector<int64_t> off(chunk + 1);
+        std::vector<int32_t> ids(chunk * n);
+        for (int t0 = 0; t0 < cycles && rc == BSIM_OK; t0 += (int)chunk) {
+            const int64_t k = std::min<int64_t>(chunk, cycles - t0);
+            rc = bsim_record(e, k, k * n);
+            if (rc == BSIM_OK) rc = bsim_trace(e, k, 0, n);
+            if (rc == BSIM_OK) rc = bsim_run(e, k);
+            int64_t ns = 0, nt = 0;
+            if (rc == BSIM_OK) rc = bsim_read_raster(e, off.data(), ids.data(), k * n, &ns);
+            if (rc == BSIM_OK)
+                rc = bsim_read_trace(e, tr.data(), tr.data() + k * n, tr.data() + 2 * k * n, tr.data() + 3 * k * n,
+                                     tr.data() + 4 * k * n, &nt);
+            if (rc != BSIM_OK) break;
+            for (int64_t c = 0; c < k; c++) {
+                for (int64_t i = (c < ns ? off[c] : 0); i < (c < ns ? off[c + 1] : 0); i++) fprintf(f[0], "%d ", ids[i]);
+                fprintf(f[0], "\n");
+                for (int q = 0; q < 5; q++) {
+                    const float *row = tr.data() + (int64_t)q * k * n + c * n;
+                    if (c < nt)
+                        for (int64_t i = 0; i < n; i++) fprintf(f[1 + q], "%.10lf \t", (double)row[i]);
+                    fprintf(f[1 + q], "\n");
+                }
             }
-            fprintf(vf, "\n");
-            fprintf(ef, "\n");
-            fprintf(jf, "\n");
         }
-        fclose(lf);
-        fclose(vf);
-        fclose(ef);
-        fclose(jf);
+        for (int k = 0; k < 6; k++)
+            if (f[k]) fclose(f[k]);
         return rc;
     }
 #endif

@@ -77,7 +77,10 @@ typedef struct bsim_options {
     int32_t build_tiles;   /* 1: also build the target-tiled copy; 0: only for TILE/AUTO; -1: never
                               (an AUTO engine then pushes every cycle; saves ~8 B per synapse) */
     int32_t tile_size;     /* target neurons per tile (0: chosen from the network size and delays, <= 5000) */
-    int32_t reserved[7];
+    int32_t lif_blocks;    /* blocks of the step kernel that run the neuron update (the others start
+                              delivering at once; both halves of a cycle touch disjoint data, so the
+                              bandwidth-bound update overlaps the delivery); 0: every block */
+    int32_t reserved[6];
 } bsim_options;
 
 /* Parameters of one generated network (see bsim_create_generated). */
@@ -198,6 +201,18 @@ int bsim_record(bsim_engine *e, int64_t max_steps, int64_t capacity);
 /* Copies the recording out: step_off [n_steps+1], ids in step order (each step's ids
  * ascending). *n_steps receives the recorded steps. BSIM_ERR_LIMIT if the buffer overflowed. */
 int bsim_read_raster(bsim_engine *e, int64_t *step_off, int32_t *ids, int64_t ids_cap, int64_t *n_steps);
+
+/* State trace of the next `max_steps` cycles: after each cycle, v, i_E, i_I and the
+ * synaptic input the cycle consumed (excitatory, inhibitory) of the neurons
+ * [first, first + count) are copied into a device buffer inside the step itself — the
+ * reference's LOG_DATA files g_v.data, g_ie.data, g_ii.data, g_input_e.data and
+ * g_input_i.data (src/sim/SingleGPUSimulator.cu:150-206), without a host copy per cycle.
+ * Calling it again restarts the trace (the buffer is kept when large enough). */
+int bsim_trace(bsim_engine *e, int64_t max_steps, int64_t first, int64_t count);
+
+/* Copies the trace out: each non-NULL array receives [n_steps][count] floats in
+ * cycle order; *n_steps the cycles traced so far. */
+int bsim_read_trace(bsim_engine *e, float *v, float *i_E, float *i_I, float *in_E, float *in_I, int64_t *n_steps);
 
 /* Neuron state: v, i_E, i_I, refrac_step per neuron (cudaFetchLIFE,
  * src/neuron/lif/GLIFENeurons.cu:29-40). Any pointer may be NULL. For input-drive

@@ -57,9 +57,20 @@ def test_sgsim_outputs_match_reference(demos, which, acc):
         subprocess.run([demos[1], str(which)], cwd=d, check=True, env=env, stdout=subprocess.DEVNULL)
         count = np.loadtxt(os.path.join(d, "GFire.count"), dtype=np.int64)
         v = np.loadtxt(os.path.join(d, "g_v.data"))
+        ie = np.loadtxt(os.path.join(d, "g_ie.data"))
+        ii = np.loadtxt(os.path.join(d, "g_ii.data"))
+        ine = np.loadtxt(os.path.join(d, "g_input_e.data"))
+        ini = np.loadtxt(os.path.join(d, "g_input_i.data"))
         raster = [np.array(line.split(), dtype=np.int32) for line in open(os.path.join(d, "GSim.log"))]
         info = open(os.path.join(d, "GSim.info")).read()
     assert "NeuronNum: 30, SynapseNum: 200" in info
+    # the per-cycle files come from the on-device trace: one line per cycle, one value per neuron
+    for arr in (v, ie, ii, ine, ini):
+        assert arr.shape == (1000, 30)
+    printed = lambda x: np.array([float("%.10f" % y) for y in np.ravel(x)])
+    assert np.abs(ie[-1] - printed(ref["final_state"][:, 1])).max() <= 1.01e-10
+    assert np.abs(ii[-1] - printed(ref["final_state"][:, 2])).max() <= 1.01e-10
+    assert ine.min() >= 0 and ini.max() <= 0
     assert np.array_equal(count, ref["fire_count"])
     assert len(raster) == 1000 and all(np.array_equal(a, b) for a, b in zip(raster, ref["raster"]))
     assert np.abs(v - GOLDEN["unit%d" % which]).max() < 3.5e-7
