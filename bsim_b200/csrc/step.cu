@@ -103,7 +103,8 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
             tr_steps = tc.steps;
         }
     }
-    for (int64_t bbase = (int64_t)blockIdx.x * blockDim.x; bbase < a.N; bbase += stride) {
+    int buf = 0;  // s_wcnt is double-buffered by pass, so a pass needs no closing barrier
+    for (int64_t bbase = (int64_t)blockIdx.x * blockDim.x; bbase < a.N; bbase += stride, buf ^= 64) {
         const int64_t base = bbase + (threadIdx.x & ~31);
         const int64_t j = base + lane;
         bool fired = false;
@@ -174,10 +175,10 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
         }
         const unsigned mask = __ballot_sync(0xffffffffu, fired);
         if (lane == 0 && base < a.N) bm[base >> 5] = mask;
-        if (lane == 0) s_wcnt[warp] = __popc(mask);
+        if (lane == 0) s_wcnt[buf + warp] = __popc(mask);
         __syncthreads();
         if (warp == 0) {
-            int c = lane < nwarps ? s_wcnt[lane] : 0;
+            int c = lane < nwarps ? s_wcnt[buf + lane] : 0;
             const int own = c;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -188,13 +189,13 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
             int at = 0;
             if (lane == 0 && total) at = atomicAdd(&a.ring_cnt[cur], total);
             at = __shfl_sync(0xffffffffu, at, 0);
-            if (lane < nwarps) s_wcnt[32 + lane] = at + c - own;  // this warp's first position
+            if (lane < nwarps) s_wcnt[buf + 32 + lane] = at + c - own;  // this warp's first position
         }
         __syncthreads();
         if (mask) {
             if (fired) {
-                slot_ids[s_wcnt[32 + warp] + __popc(mask & ((1u << lane) - 1u))] = (int32_t)j;
-                a.fire_count[j] += 1;
+                slot_ids[s_wcnt[buf + 32 + warp] + __popc(mask & ((1u << lane) - 1u))] = (int32_t)j;
+                atomicAdd(&a.fire_count[j], 1);  // a reduction: nothing waits for the old count
             }
             if (hist) {
                 // one atomic per (warp, population) with spikes
@@ -202,8 +203,10 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
                 if (fired && lane == __ffs(same) - 1) atomicAdd(&hist[pop], __popc(same));
             }
         }
-        __syncthreads();  // s_wcnt is reused by the next pass
+        // no barrier here: the next pass writes the other half of s_wcnt, and the pass
+        // after it is ordered by the next pass's two barriers
     }
+    __syncthreads();  // s_wcnt is free for the caller
 }
 
 // ---------------------------------------------------------------------------
@@ -798,7 +801,7 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const __grid
 {
     __shared__ long long s_cum[BSIM_MAX_DELAY + 1];
     __shared__ PushSeg s_seg[MAX_WARPS * PUSH_CHUNK];
-    __shared__ int s_wcnt[64];
+    __shared__ int s_wcnt[128];
     __shared__ unsigned long long s_ev;
     __shared__ __align__(8) int s_part[4];  // tiled delivery: the block's part; [2..3] the best part to join
     __shared__ int s_last;
