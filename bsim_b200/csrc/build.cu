@@ -719,6 +719,14 @@ static int build_tiles_host(Engine &e, const int32_t *inst, const int32_t *pop, 
     th.tile_scale.resize(nt);
     for (int32_t q = 0; q < nt; q++) th.tile_scale[q] = ldexpf(1.0f, e.qexp[inst ? inst[th.tile_beg[q]] : 0]);
     th.tile_run_off.assign(nt + 1, 0);
+    // a tile scans the delay slots of its own network's longest delay only, so
+    // networks with short delays packed beside long-delay ones do not pay for them
+    std::vector<int32_t> dmax_inst(std::max<int32_t>(1, e.n_inst), 1);
+    for (int64_t k = 0; k < s; k++) {
+        int32_t &dm = dmax_inst[inst ? inst[src[k]] : 0];
+        dm = std::max(dm, delay[k]);
+    }
+    auto tile_D = [&](int32_t q) { return dmax_inst[inst ? inst[th.tile_beg[q]] : 0]; };
     std::vector<int64_t> pair_base;
     std::vector<uint16_t> pair_doff;
     std::vector<uint2> ent;
@@ -746,7 +754,8 @@ static int build_tiles_host(Engine &e, const int32_t *inst, const int32_t *pop, 
         std::fill(cnt.begin(), cnt.end(), 0);
     };
     auto close_run = [&]() {
-        if (run_start_src >= 0) add_run(th, (uint32_t)run_start_src, (int32_t)(cur_src - run_start_src + 1), run_pair0, D);
+        if (run_start_src >= 0)
+            add_run(th, (uint32_t)run_start_src, (int32_t)(cur_src - run_start_src + 1), run_pair0, tile_D(cur_tile));
     };
     auto open_tiles_until = [&](int32_t q) {
         while ((int32_t)th.tile_units.size() <= q) {
@@ -1272,7 +1281,7 @@ static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, co
                     sg.d_inst = x.D;
                     sg.sign = -1;
                     segs.push_back(sg);
-                    add_run(th, (uint32_t)sg.src_base, x.n, pairs, D);
+                    add_run(th, (uint32_t)sg.src_base, x.n, pairs, x.D);  // the network's own delay range
                     pairs += x.n;
                 }
             }
