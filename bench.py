@@ -468,6 +468,11 @@ def predicted_vs_plain(steps, device, settle=1000, chunk=50):
         eng.set_predictor(params, tolerance=0.3, cost_push=cost_push, cost_tile=cost_tile)
 
     ev_a, _, ms_a, _, fc_a, st = run_mode(B.DELIVERY_AUTO, attach)
+
+    def attach_exact(eng):
+        eng.set_predictor(None, cost_push=cost_push, cost_tile=cost_tile)
+
+    ev_x, _, ms_x, _, fc_x, st_x = run_mode(B.DELIVERY_AUTO, attach_exact)
     n_net = sp.n_pop * sp.pop_size
     rate = sp_p / chunk / n_net / DT
     eps = lambda ev, ms: float(ev.sum() / (ms.sum() / 1e3))
@@ -478,12 +483,16 @@ def predicted_vs_plain(steps, device, settle=1000, chunk=50):
             "rate_hz_low_high": [float(rate[~hi_p].mean()) if (~hi_p).any() else None,
                                  float(rate[hi_p].mean()) if hi_p.any() else None],
             "events_per_s": {"push": eps(ev_p, ms_p), "tile": eps(ev_t, ms_t), "auto_predicted": eps(ev_a, ms_a),
+                             "auto_exact": eps(ev_x, ms_x),
                              "best_fixed_per_chunk": float(ev_p.sum() / (ideal / 1e3))},
             "ms_per_cycle": {"push": float(ms_p.sum() / steps), "tile": float(ms_t.sum() / steps),
-                             "auto_predicted": float(ms_a.sum() / steps)},
-            "hbm_roofline_frac": {"push": frac(ev_p, ms_p), "tile": frac(ev_t, ms_t), "auto_predicted": frac(ev_a, ms_a)},
+                             "auto_predicted": float(ms_a.sum() / steps), "auto_exact": float(ms_x.sum() / steps)},
+            "hbm_roofline_frac": {"push": frac(ev_p, ms_p), "tile": frac(ev_t, ms_t), "auto_predicted": frac(ev_a, ms_a),
+                                  "auto_exact": frac(ev_x, ms_x)},
             "cost_models_ns": {"push": cost_push, "tile": cost_tile, "form": "a + b * events per cycle"},
-            "spike_counts_identical": bool(np.array_equal(fc_p, fc_t) and np.array_equal(fc_p, fc_a)),
+            "auto_exact_tile_cycles": int(st_x.tile_cycles),
+            "spike_counts_identical": bool(np.array_equal(fc_p, fc_t) and np.array_equal(fc_p, fc_a)
+                                           and np.array_equal(fc_p, fc_x)),
             "predictor": {"train_loss": loss, "train_seconds": t_train, "cycles": int(st.cycles),
                           "fallbacks": int(st.fallbacks), "fallback_rate": st.fallbacks / max(st.cycles, 1),
                           "tile_cycles": int(st.tile_cycles),

@@ -1944,28 +1944,37 @@ int bsim_set_predictor(bsim_engine *eh, const float *params, float tolerance, co
     Engine &e = *H(eh);
     CK(cudaSetDevice(e.device));
     CK(cudaStreamSynchronize(e.stream));
-    if (!params) {
+    if (!params && !cost_push && !cost_tile) {  // detached: AUTO pushes every cycle
         e.a.mlp = nullptr;
+        e.a.pstats = nullptr;
         drop_graph(e);
         return BSIM_OK;
     }
-    if (!e.a.pop_hist) return fail(BSIM_ERR_STATE, "bsim_set_predictor: enable population statistics first");
-    if (!e.a.pred_ring) {
-        float *w, *ring, *sum;
+    if (params && !e.a.pop_hist) return fail(BSIM_ERR_STATE, "bsim_set_predictor: enable population statistics first");
+    if (!e.pstats_mem) {
         PredStats *ps;
-        TRY(dalloc(e, &w, BSIM_MLP_PARAMS));
-        TRY(dalloc(e, &ring, 4 * (size_t)e.n_pops));
-        TRY(dalloc(e, &sum, 8));
         TRY(dalloc(e, &ps, 1));
-        e.a.mlp = w;
-        e.a.pred_ring = ring;
-        e.a.pred_sum = sum;
-        e.a.pstats = ps;
+        e.pstats_mem = ps;
     }
-    CK(cudaMemcpy(const_cast<float *>(e.a.mlp), params, sizeof(float) * BSIM_MLP_PARAMS, cudaMemcpyHostToDevice));
-    CK(cudaMemset(e.a.pred_ring, 0, sizeof(float) * 4 * e.n_pops));
-    CK(cudaMemset(e.a.pred_sum, 0, sizeof(float) * 8));
+    e.a.pstats = e.pstats_mem;
     CK(cudaMemset(e.a.pstats, 0, sizeof(PredStats)));
+    if (!params) {  // the exact schedule: the cost models on the delivered window's spike count
+        e.a.mlp = nullptr;
+    } else {
+        if (!e.mlp_mem) {
+            float *w, *ring, *sum;
+            TRY(dalloc(e, &w, BSIM_MLP_PARAMS));
+            TRY(dalloc(e, &ring, 4 * (size_t)e.n_pops));
+            TRY(dalloc(e, &sum, 8));
+            e.mlp_mem = w;
+            e.a.pred_ring = ring;
+            e.a.pred_sum = sum;
+        }
+        e.a.mlp = e.mlp_mem;
+        CK(cudaMemcpy(e.mlp_mem, params, sizeof(float) * BSIM_MLP_PARAMS, cudaMemcpyHostToDevice));
+        CK(cudaMemset(e.a.pred_ring, 0, sizeof(float) * 4 * e.n_pops));
+        CK(cudaMemset(e.a.pred_sum, 0, sizeof(float) * 8));
+    }
     e.a.pred_tol = tolerance;
     e.a.mean_outdeg = e.N ? (float)((double)e.S / (double)e.N) : 0.0f;
     e.a.cost_push_a = cost_push ? cost_push[0] : 0.0f;

@@ -180,6 +180,10 @@ struct Engine {
     // staging for state uploads and read-backs: four planes of N words (v, i_E,
     // i_I, refrac), so the host's arrays move with one copy each, no host repacking
     float *stage = nullptr;
+    // schedule state: predictor statistics and the MLP's parameters (a.pstats / a.mlp
+    // point here while a schedule / a predictor is attached)
+    PredStats *pstats_mem = nullptr;
+    float *mlp_mem = nullptr;
     // population statistics (device arrays in a: pop_size, pop_indeg, pop_outdeg)
     bool pop_info_ready = false;
     // tiled copy, host side: synapses and work units per tile (planning the parts)

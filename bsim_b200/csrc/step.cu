@@ -756,12 +756,41 @@ static __device__ __forceinline__ void predict_phase(const StepArgs &a, unsigned
     }
 }
 
-// The delivery mode of cycle t under BSIM_DELIVERY_AUTO: the cost model on the
-// predicted work, or on the exact spike count of cycle t-1 when the prediction
-// for that cycle missed by more than the tolerance (the fallback). Every block
-// computes the same choice from the same device words.
+// Spikes of the cycles a step delivers (t-1 .. t-D), from the ring counts; every
+// lane of the calling warp gets the sum.
+static __device__ __forceinline__ float window_spikes(const StepArgs &a, unsigned long long t)
+{
+    const int lane = threadIdx.x & 31;
+    float c = 0.0f;
+    for (int d = 1 + lane; d <= a.D; d += 32)
+        if ((long long)t - d >= 0) c += (float)a.ring_cnt[(t - d) % (unsigned long long)a.R];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    return c;
+}
+
+// The delivery mode of cycle t under BSIM_DELIVERY_AUTO: the cost model of each
+// mode (fixed ns per cycle + ns per event) on the cycle's work.
+//  * exact schedule (no predictor attached): the work is the exact spike count of
+//    the delivered window t-1 .. t-D times the mean out-degree over D (each spike's
+//    synapses are spread over the D delays);
+//  * learned schedule: the work is the predictor's estimate for cycle t-1's spikes
+//    times the mean out-degree, or the exact count of cycle t-1 when the prediction
+//    for that cycle missed by more than the tolerance (the fallback).
+// Every block computes the same choice from the same device words.
 static __device__ __forceinline__ int auto_delivery(const StepArgs &a, unsigned long long t)
 {
+    if (!a.mlp) {
+        const float work = window_spikes(a, t) * a.mean_outdeg / (float)a.D;
+        const int dm = (a.n_tiles > 0 && a.cost_tile_a + a.cost_tile_b * work < a.cost_push_a + a.cost_push_b * work)
+                           ? BSIM_DELIVERY_TILE
+                           : BSIM_DELIVERY_PUSH;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            a.pstats->cycles += 1;
+            a.pstats->tile_cycles += dm == BSIM_DELIVERY_TILE ? 1 : 0;
+        }
+        return dm;
+    }
     float ps = 0.0f, pe = 0.0f, as = 0.0f;
     if (t >= 1) {
         const float *slot = a.pred_sum + ((t - 1) & 3) * 2;
@@ -827,7 +856,7 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const __grid
     const int p = (int)(t & 1ull);
     const int cur = (int)(t % (unsigned long long)a.R);
     int dm = a.deliv_sel ? *a.deliv_sel : a.delivery;
-    if (dm == BSIM_DELIVERY_AUTO) dm = a.mlp ? auto_delivery(a, t) : BSIM_DELIVERY_PUSH;
+    if (dm == BSIM_DELIVERY_AUTO) dm = a.pstats ? auto_delivery(a, t) : BSIM_DELIVERY_PUSH;
     if (dm == BSIM_DELIVERY_TILE && a.n_tiles == 0) dm = BSIM_DELIVERY_PUSH;
     if (a.mlp && blockIdx.x == 0 && threadIdx.x == 32) {
         // slot t+2 is next written by cycle t+1's prediction

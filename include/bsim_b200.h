@@ -274,12 +274,18 @@ int bsim_mlp_grad(const float *params, const float *x, const float *y_target, in
 int bsim_mlp_train(float *params, const float *x, const float *y_target, int64_t n, int32_t epochs, int32_t batch,
                    float lr, uint64_t seed, float *final_loss);
 
-/* Attaches (params != NULL) or detaches (NULL) the predictor. Needs population
- * statistics. With delivery BSIM_DELIVERY_AUTO the predicted events of the next
- * cycle pick push or tiled delivery by the cost model (ns per event and fixed ns
- * per cycle of each mode, e.g. from bsim_autotune); when the exact spike count of a
- * cycle departs from its prediction by more than tolerance (relative), that
- * cycle's choice is recomputed from the exact counts (a fallback). */
+/* Sets the schedule of BSIM_DELIVERY_AUTO: each cycle picks push or tiled delivery by
+ * the cost models (fixed ns per cycle and ns per event of each mode, e.g. from
+ * bsim_autotune or a fit over plain runs) applied to the cycle's work.
+ *   params != NULL: the learned schedule (needs population statistics): the work is the
+ *     predicted events of the last cycle; when a cycle's exact spike count departs from
+ *     its prediction by more than tolerance (relative), its choice is recomputed from
+ *     the exact count (a fallback).
+ *   params == NULL with cost models: the exact schedule: the work is the exact spike
+ *     count of the delivered window (the last max_delay cycles) times the mean
+ *     out-degree over max_delay. A step delivers only spikes of past cycles, so its
+ *     work is known before it starts.
+ *   all NULL: detached; AUTO then pushes every cycle. */
 int bsim_set_predictor(bsim_engine *e, const float *params, float tolerance, const float *cost_push,
                        const float *cost_tile);
 

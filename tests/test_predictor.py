@@ -191,3 +191,32 @@ def test_auto_without_tiled_copy_pushes_every_cycle(trained):
     assert auto.predictor_stats().tile_cycles == 0
     with pytest.raises(B.BsimError):
         B.Engine.generated(sp, DT, opts=B.options(delivery=B.DELIVERY_TILE, build_tiles=-1))
+
+
+@pytest.mark.gpu
+def test_exact_schedule_switches_modes_and_keeps_dynamics():
+    """AUTO delivery under the exact schedule (no predictor: the cost models on the
+    delivered window's exact spike count) on a square-wave-driven network: both
+    modes are used and the spikes equal the plain push run's."""
+    import bsim_b200 as B
+    from bsim_b200 import workloads as W
+    sp = W.cuba(8, 600, 500, 20, seed=71, i_max=2.5e-9)
+    sp.drive_scale, sp.drive_half_period = 32.0, 100
+    dt = np.float32(1e-4)
+    plain = B.Engine.generated(sp, dt)
+    plain.record(600, 600 * 4800)
+    plain.run(600)
+    spikes = np.array([len(r) for r in plain.raster()], np.float64)
+    # the exact schedule's work: the mean spikes of the delivered window (20 cycles)
+    # times the mean out-degree; put the crossover at the median window
+    win = np.array([spikes[max(0, t - 20):t].sum() / 20.0 for t in range(600)])
+    auto = B.Engine.generated(sp, dt, opts=B.options(delivery=B.DELIVERY_AUTO))
+    inf = auto.info()
+    work = float(np.median(win[20:])) * inf.n_synapses / inf.n_neurons
+    auto.set_predictor(None, cost_push=[0.0, 1.0], cost_tile=[work, 0.0])
+    auto.run(600)
+    st = auto.predictor_stats()
+    assert st.cycles == 600 and st.fallbacks == 0
+    assert 60 < st.tile_cycles < 540
+    assert np.array_equal(auto.fire_count(), plain.fire_count())
+    assert np.array_equal(auto.state()["v"], plain.state()["v"])
