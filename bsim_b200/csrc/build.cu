@@ -667,26 +667,54 @@ static int upload_tiles(Engine &e, const TileHost &th)
     return BSIM_OK;
 }
 
-// Segment starts of every (pair, delay) in 16-byte entry pairs, from the pair
-// offsets and the per-delay cumulative counts (all even).
-__global__ void pair_seg_kernel(const int64_t *pair_base, const uint16_t *pair_doff, int64_t n_pairs, int D,
-                                uint32_t *pair_seg)
+// Segment starts of every (pair, delay) in 16-byte entry pairs, relative to the
+// first entry pair of the pair's tile (so each tile, not the whole copy, must
+// stay below 2^32 entry pairs), from the pair offsets and the per-delay
+// cumulative counts (all even).
+__global__ void tile_seg0_kernel(const int64_t *pair_base, const int64_t *tile_pair0, int32_t nt, int64_t n_pairs,
+                                 int64_t *tile_seg0)
 {
-    const int64_t n = n_pairs * (D + 1);
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        pair_seg[i] = (uint32_t)((pair_base[i / (D + 1)] + pair_doff[i]) >> 1);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nt; q += gridDim.x * blockDim.x)
+        tile_seg0[q] = tile_pair0[q] < n_pairs ? (pair_base[tile_pair0[q]] >> 1) : 0;
 }
 
-static int make_pair_seg(Engine &e, int64_t n_pairs, int64_t n_entries)
+__global__ void pair_seg_kernel(const int64_t *pair_base, const uint16_t *pair_doff, int64_t n_pairs, int D,
+                                const int64_t *tile_pair0, int32_t nt, const int64_t *tile_seg0, uint32_t *pair_seg)
 {
-    if (n_entries / 2 > (int64_t)UINT32_MAX) return fail(BSIM_ERR_LIMIT, "tiled delivery: more than 2^33 entries");
+    const int64_t n = n_pairs * (D + 1);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = i / (D + 1);
+        int lo = 0, hi = nt - 1;  // the tile whose pair range holds k
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (tile_pair0[mid] <= k) lo = mid;
+            else hi = mid - 1;
+        }
+        pair_seg[i] = (uint32_t)(((pair_base[k] + pair_doff[i]) >> 1) - tile_seg0[lo]);
+    }
+}
+
+// tile_pair0: [nt + 1] first pair of each tile (pairs are grouped by tile).
+static int make_pair_seg(Engine &e, int64_t n_pairs, const std::vector<int64_t> &tile_pair0)
+{
+    const int32_t nt = (int32_t)tile_pair0.size() - 1;
+    for (int32_t q = 0; q < nt && q < (int32_t)e.tile_entries.size(); q++)
+        if (e.tile_entries[q] / 2 > (int64_t)UINT32_MAX)
+            return fail(BSIM_ERR_LIMIT, "tiled delivery: a tile with more than 2^33 entries");
     uint32_t *d_seg;
+    int64_t *d_seg0, *d_tp0;
     TRY(dalloc(e, &d_seg, (size_t)n_pairs * (e.D + 1)));
-    if (n_pairs > 0)
-        pair_seg_kernel<<<e.sm_count * 4, 256, 0, e.stream>>>(e.a.pair_base, e.a.pair_doff, n_pairs, e.D, d_seg);
+    TRY(dalloc(e, &d_seg0, std::max<int32_t>(nt, 1)));
+    TRY(dalloc(e, &d_tp0, nt + 1));
+    CK(cudaMemcpy(d_tp0, tile_pair0.data(), sizeof(int64_t) * (nt + 1), cudaMemcpyHostToDevice));
+    if (nt > 0) tile_seg0_kernel<<<e.sm_count, 256, 0, e.stream>>>(e.a.pair_base, d_tp0, nt, n_pairs, d_seg0);
+    if (n_pairs > 0 && nt > 0)
+        pair_seg_kernel<<<e.sm_count * 4, 256, 0, e.stream>>>(e.a.pair_base, e.a.pair_doff, n_pairs, e.D, d_tp0, nt,
+                                                             d_seg0, d_seg);
     CK(cudaStreamSynchronize(e.stream));
     CK(cudaGetLastError());
     e.a.pair_seg = d_seg;
+    e.a.tile_seg0 = d_seg0;
     return BSIM_OK;
 }
 
@@ -811,7 +839,11 @@ static int build_tiles_host(Engine &e, const int32_t *inst, const int32_t *pop, 
     e.a.pair_base = d_pb;
     e.a.pair_doff = d_pd;
     e.a.ent = d_ent;
-    TRY(make_pair_seg(e, (int64_t)pair_base.size(), (int64_t)ent.size()));
+    // pairs are grouped by tile: a tile's first pair is its first run's
+    std::vector<int64_t> tile_pair0(nt + 1, (int64_t)pair_base.size());
+    for (int32_t q = nt - 1; q >= 0; q--)
+        tile_pair0[q] = th.tile_run_off[q] < th.tile_run_off[q + 1] ? th.run_pair0[th.tile_run_off[q]] : tile_pair0[q + 1];
+    TRY(make_pair_seg(e, (int64_t)pair_base.size(), tile_pair0));
     return upload_tiles(e, th);
 }
 
@@ -1324,7 +1356,7 @@ static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, co
         E.a.pair_base = d_pb;
         E.a.pair_doff = d_pd;
         E.a.ent = d_ent;
-        if ((rc = make_pair_seg(E, pairs, n_ent))) { free_tmp(); return bail(rc); }
+        if ((rc = make_pair_seg(E, pairs, tile_pair0))) { free_tmp(); return bail(rc); }
         if ((rc = upload_tiles(E, th))) { free_tmp(); return bail(rc); }
     }
     // push rows (not needed when every step uses the tiled copy)

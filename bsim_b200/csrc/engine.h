@@ -132,8 +132,10 @@ struct StepArgs {
     const int32_t *run_unit0;        // [runs] first work unit, counted within the tile
     const int64_t *pair_base;        // [P] first entry of each pair
     const uint16_t *pair_doff;       // [P][D + 1] cumulative entry counts by delay (padded to even)
-    const uint32_t *pair_seg;        // [P][D + 1] each delay's segment start in 16-byte entry pairs
-                                     // (pair_base + pair_doff) / 2; the last one is the pair's end
+    const uint32_t *pair_seg;        // [P][D + 1] each delay's segment start in 16-byte entry pairs,
+                                     // (pair_base + pair_doff) / 2 - tile_seg0[tile]; the last one is
+                                     // the pair's end
+    const int64_t *tile_seg0;        // [n_tiles] first 16-byte entry pair of each tile
     const uint2 *ent;                // [E] {target within the tile, weight bits}; every (pair, delay)
                                      // segment starts on an even entry and has even length
                                      // (padding entries have target 0xffffffff)

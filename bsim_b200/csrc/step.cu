@@ -539,6 +539,7 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
         for (int i = threadIdx.x; i < 4 * T; i += blockDim.x) s_acc[i] = 0u;
         __syncthreads();
         const float sc = a.tile_scale[q];
+        const long long seg0 = a.tile_seg0[q];  // the tile's first entry pair
         const int r0 = a.tile_run_off[q], r1 = a.tile_run_off[q + 1];
         // the warps of every block working on the part take chunks of its units as they become
         // free: 32 units (one per lane), fewer where the part listed many entry pairs per unit in
@@ -607,7 +608,7 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
 #pragma unroll
                     for (int u = 0; u < 4; u++) {
                         if (i0 + u < take) {
-                            seg_start[excl + i0 + u] = sg[u].x;
+                            seg_start[excl + i0 + u] = seg0 + (long long)sg[u].x;
                             seg_cum[excl + i0 + u] = (int)(sg[u].y - sg[u].x);  // length for now
                         }
                     }
