@@ -62,3 +62,33 @@ def test_cpu_baseline_runs_reference_copies_on_a_small_replica():
     else:
         assert info["kind"] == "port" and info["copies"] == 1
     assert "replica" in info["sample"] and info["replica_synapses"] > 0
+
+
+class _FakeEngine:
+    """Events per cycle rising linearly for `rise` cycles, then flat (a start-up transient)."""
+
+    class _Info:
+        pass
+
+    def __init__(self, rise, level=1000.0):
+        self.t, self.ev, self.rise, self.level = 0, 0.0, rise, level
+
+    def run(self, k):
+        for _ in range(k):
+            self.ev += self.level * min(1.0, self.t / self.rise)
+            self.t += 1
+
+    def info(self):
+        i = self._Info()
+        i.events_total = self.ev
+        return i
+
+
+def test_settle_waits_for_the_transient_and_stops_when_flat():
+    done, per_chunk = bench.settle(_FakeEngine(4000), 3000, 10000)
+    assert 4000 + 4 * 250 <= done < 10000          # past the rise by a window (3 % tolerance)
+    assert per_chunk[-1] == pytest.approx(1000.0)
+    done, _ = bench.settle(_FakeEngine(100), 3000, 10000)
+    assert done == 3000                             # already flat: the minimum
+    done, _ = bench.settle(_FakeEngine(10 ** 9), 3000, 10000)
+    assert done == 10000                            # still rising: the maximum
