@@ -134,3 +134,57 @@ def test_drive_program_fire_count_matches_oracle(drive_demo):
     assert "NeuronTypeNum: 3" in info
     assert np.array_equal(count, ref["fire_count"])
     assert ref["fire_count"][10:].sum() > 0
+
+
+# ---------------------------------------------------------------------------
+# The reference's own example programs, compiled unchanged against include/BSim.h
+# by `make -C oracle refprogs` (part of the build where the reference's sources are
+# present): test/gpu/lif_unit{1..4}_test.cpp and test/gpu/standard_test.cpp.
+# ---------------------------------------------------------------------------
+PROGS = os.path.join(ROOT, "oracle", "_ref", "progs")
+needs_progs = pytest.mark.skipif(not os.path.exists(os.path.join(PROGS, "standard_test.log")),
+                                 reason="the reference's programs were not built (no reference sources)")
+
+
+@pytest.mark.gpu
+@needs_progs
+@pytest.mark.parametrize("which", [1, 2, 3, 4])
+def test_reference_unit_programs_unchanged(which):
+    """lif_unit{k}_test.cpp of the reference, built with -DLOG_DATA: its g_v.data
+    matches the reference's golden trace test/lif_unit{k}_test_v.std, its raster and
+    GFire.count the oracle's."""
+    ref = oracle_unit(which)
+    with tempfile.TemporaryDirectory() as d:
+        subprocess.run([os.path.join(PROGS, "lif_unit%d_test.log" % which)], cwd=d, check=True,
+                       stdout=subprocess.DEVNULL)
+        v = np.loadtxt(os.path.join(d, "g_v.data"))
+        raster = [np.array(line.split(), dtype=np.int32) for line in open(os.path.join(d, "GSim.log"))]
+        info = open(os.path.join(d, "GSim.info")).read()
+    assert "NeuronNum: 30, SynapseNum: 200" in info
+    assert v.shape == (1000, 30) and np.abs(v - GOLDEN["unit%d" % which]).max() < 3.5e-7
+    assert len(raster) == 1000 and all(np.array_equal(a, b) for a, b in zip(raster, ref["raster"]))
+
+
+@pytest.mark.gpu
+@needs_progs
+def test_reference_standard_test_program_unchanged():
+    """standard_test.cpp of the reference (the all-to-all chain of its README's
+    benchmark, 5 % preset) on a small depth: it builds, runs 1,000 cycles and writes
+    the reference's output files; the network it builds has the size the program
+    implies; ordered and exact accumulation (which differ only in rounding) give
+    total spike counts within 5 % of each other."""
+    depth, n = 8, 200
+    counts = {}
+    for acc in ("ordered", "exact"):
+        with tempfile.TemporaryDirectory() as d:
+            env = dict(os.environ, BSIM_ACCUMULATE=acc)
+            subprocess.run([os.path.join(PROGS, "standard_test"), str(depth), str(n), "0.7", "0.9", "0.6", "0.2", "6"],
+                           cwd=d, check=True, env=env, stdout=subprocess.DEVNULL)
+            info = open(os.path.join(d, "GSim.info")).read()
+            counts[acc] = np.loadtxt(os.path.join(d, "GFire.count"), dtype=np.int64)
+    side = len(range(1, depth, 4))                  # inhibitory side populations
+    conns = (depth - 1) + (depth // 6) + 2 * side  # chain, g1 -> g[i] for i % 6 == 0, side pairs
+    assert "NeuronNum: %d, SynapseNum: %d" % ((depth + side) * n, conns * n * n) in info
+    assert counts["exact"].shape == ((depth + side) * n,)
+    assert counts["exact"].sum() > 0
+    assert abs(int(counts["exact"].sum()) - int(counts["ordered"].sum())) <= 0.05 * counts["ordered"].sum()
