@@ -513,6 +513,44 @@ def dense_leg(steps, device, settle_min=1000):
                          "alg_bytes_per_launch": alg}}
 
 
+def reference_program_leg(depth=120, n=1000, preset=("0.7", "0.5", "0.6", "0.3", "6")):
+    """The reference's own benchmark program, test/gpu/standard_test.cpp, compiled unchanged
+    against include/BSim.h (oracle/_ref/progs, built where the reference's sources are
+    present), run on the case its source comments time on a P100: depth 120, 1,000
+    neurons per population, the 2 % preset, 1,000 cycles. Its GSim.info loop time (the
+    same gettimeofday window as the reference's) is set beside the published 0.432303 s
+    (test/gpu/standard_test.cpp:22,29-30,43; other hardware, depth unspecified there
+    within 120-300)."""
+    prog = os.path.join(ROOT, "oracle", "_ref", "progs", "standard_test")
+    if not os.path.exists(prog):
+        return {"unavailable": "the reference's programs were not built (no reference sources at build time)"}
+    out = {"program": "standard_test %d %d %s" % (depth, n, " ".join(preset)), "cycles": 1000,
+           "p100_published_loop_seconds": 0.432303}
+    for deliv in ("push", "tile"):
+        with tempfile.TemporaryDirectory() as d:
+            env = dict(os.environ, BSIM_DELIVERY=deliv)
+            t0 = time.perf_counter()
+            r = subprocess.run([prog, str(depth), str(n)] + list(preset), cwd=d, env=env, capture_output=True,
+                               text=True, timeout=600)
+            wall = time.perf_counter() - t0
+            if r.returncode != 0:
+                out[deliv] = {"error": r.stderr[-300:]}
+                continue
+            info = open(os.path.join(d, "GSim.info")).read()
+            loop = None
+            for line in info.splitlines():
+                if line.startswith("Simulation fin"):
+                    h, m, sec = line.split("in", 1)[1].strip().rstrip("s").split(":")
+                    loop = 3600 * int(h) + 60 * int(m) + float(sec)
+            nums = [x for x in info.replace(",", " ").split() if x.isdigit()]
+            counts = np.loadtxt(os.path.join(d, "GFire.count"), dtype=np.int64)
+            out[deliv] = {"loop_seconds": loop, "program_wall_seconds": wall,
+                          "speedup_vs_p100": 0.432303 / loop if loop else None,
+                          "spikes": int(counts.sum()), "neurons": int(counts.shape[0]),
+                          "info": " ".join(info.split())[:200]}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -529,6 +567,8 @@ def main():
     ap.add_argument("--dense-steps", type=int, default=200,
                     help="timed cycles of the dense-firing leg (50 x 20,000, ~2 kHz, delays 1-50; 0 skips it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-program", action="store_true",
+                    help="skip the reference's standard_test program (depth 120, 1,000 neurons, 2 %% preset)")
     ap.add_argument("--batched-nets", type=int, default=256,
                     help="networks in the batched+predicted vs plain comparison (0 skips it)")
     ap.add_argument("--batched-steps", type=int, default=500)
@@ -675,6 +715,12 @@ def main():
             dense = dense_leg(args.dense_steps, local)
         except Exception as ex:
             dense = {"error": str(ex)}
+    refprog = None
+    if rank == 0 and world == 1 and not args.no_reference_program:
+        try:
+            refprog = reference_program_leg()
+        except Exception as ex:
+            refprog = {"error": str(ex)}
     pred = None
     if rank == 0 and world == 1 and args.predicted_steps > 0:
         try:
@@ -697,7 +743,7 @@ def main():
                 "events_per_step": events_all / args.steps / world,
                 "mean_rate_hz": spikes_all / n_all / (args.steps * DT),
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
-                "gpu_launches": args.steps, "dense_c2": dense, "batched_vs_plain": cmp,
+                "gpu_launches": args.steps, "dense_c2": dense, "reference_program_standard_test": refprog, "batched_vs_plain": cmp,
                 "predictor_scheduled_vs_plain": pred}
         print(json.dumps(line))
     if dist:
