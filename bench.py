@@ -540,9 +540,8 @@ def reference_program_leg(depth=120, n=1000, preset=("0.7", "0.5", "0.6", "0.3",
             loop = None
             for line in info.splitlines():
                 if line.startswith("Simulation fin"):
-                    h, m, sec = line.split("in", 1)[1].strip().rstrip("s").split(":")
+                    h, m, sec = line.rsplit(" in ", 1)[1].strip().rstrip("s").split(":")
                     loop = 3600 * int(h) + 60 * int(m) + float(sec)
-            nums = [x for x in info.replace(",", " ").split() if x.isdigit()]
             counts = np.loadtxt(os.path.join(d, "GFire.count"), dtype=np.int64)
             out[deliv] = {"loop_seconds": loop, "program_wall_seconds": wall,
                           "speedup_vs_p100": 0.432303 / loop if loop else None,
