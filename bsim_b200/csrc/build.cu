@@ -1580,6 +1580,7 @@ int bsim_record(bsim_engine *eh, int64_t max_steps, int64_t capacity)
         e.rec_dirty = true;
         // the read-back's sorted copy and sort scratch, sized for a full recording
         // (recordings of 2^31 ids or more are sorted on the host and need neither)
+        e.rec_sorted = nullptr;  // the old sorted copy is too small for the new buffers
         if (cap < ((int64_t)1 << 31) && stp < ((int64_t)1 << 31)) {
             TRY(dalloc(e, &sorted, cap));
             e.rec_sorted = sorted;
