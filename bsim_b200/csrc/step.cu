@@ -499,6 +499,9 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
     int *seg_cum = s_cum + warp * TILE_SEGS;
     unsigned long long ev = 0;
     unsigned long long *s_best = reinterpret_cast<unsigned long long *>(s_part + 2);
+    // the counters start at zero once per launch; each part's flush clears what it read,
+    // so the next part (any tile size up to tile_max) finds them zero
+    for (int i = threadIdx.x; i < 4 * a.tile_max; i += blockDim.x) s_acc[i] = 0u;
     for (;;) {
         if (threadIdx.x == 0) {
             const unsigned q = atomicAdd(a.part_ctr, 1u);
@@ -536,8 +539,6 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
         const int4 part = a.parts[pi];  // {tile, first unit, end unit, plane}
         const int q = part.x, u_end = part.z;
         const int tb = a.tile_beg[q], T = a.tile_beg[q + 1] - tb;
-        for (int i = threadIdx.x; i < 4 * T; i += blockDim.x) s_acc[i] = 0u;
-        __syncthreads();
         const float sc = a.tile_scale[q];
         const long long seg0 = a.tile_seg0[q];  // the tile's first entry pair
         const int r0 = a.tile_run_off[q], r1 = a.tile_run_off[q + 1];
@@ -681,19 +682,22 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
         if (!helper) {
             // the owner stores the part's plane of the tile's {E, I} accumulator pairs
             longlong2 *g = reinterpret_cast<longlong2 *>(a.acc) + ((int64_t)pw * a.n_planes + part.w) * a.N + tb;
-            for (int i = threadIdx.x; i < T; i += blockDim.x)
+            for (int i = threadIdx.x; i < T; i += blockDim.x) {
                 g[i] = make_longlong2(carry_sum(s_acc + i, T), carry_sum(s_acc + 2 * T + i, T));
+                s_acc[i] = s_acc[T + i] = s_acc[2 * T + i] = s_acc[3 * T + i] = 0u;
+            }
         } else {
             // a helper adds what it summed into the help plane
             unsigned long long *g = reinterpret_cast<unsigned long long *>(a.acc) +
                                     2 * (((int64_t)pw * a.n_planes + a.help_plane) * a.N + tb);
             for (int i = threadIdx.x; i < T; i += blockDim.x) {
                 const long long e = carry_sum(s_acc + i, T), v = carry_sum(s_acc + 2 * T + i, T);
+                s_acc[i] = s_acc[T + i] = s_acc[2 * T + i] = s_acc[3 * T + i] = 0u;
                 if (e) red_add_u64(g + 2 * i, (unsigned long long)e);
                 if (v) red_add_u64(g + 2 * i + 1, (unsigned long long)v);
             }
         }
-        // the next part's queue read (two barriers) orders the reuse of s_acc
+        // the next part's queue read (two barriers) orders the flush before the counters' reuse
     }
     return ev;
 }
