@@ -25,7 +25,7 @@ cudaError_t launch_step(Engine &e);
 cudaError_t launch_record_flush(Engine &e);
 cudaError_t step_occupancy(int block, int accumulate, int *blocks_per_sm);
 cudaError_t step_occupancy(int block, int accumulate, int *blocks_per_sm, size_t smem);
-size_t step_dynamic_smem(const StepArgs &a);
+size_t step_dynamic_smem(const StepArgs &a, int block);
 cudaError_t step_set_smem(int accumulate, size_t bytes);
 
 static thread_local std::string g_err;
@@ -545,7 +545,7 @@ static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
     // loops of both phases see every SM
     e.block = e.opt.block_threads > 0 ? e.opt.block_threads : 512;
     if (e.block % 32 != 0 || e.block > 512) return fail(BSIM_ERR_ARG, "block_threads must be a multiple of 32 <= 512");
-    const size_t smem = step_dynamic_smem(a);
+    const size_t smem = step_dynamic_smem(a, e.block);
     if (smem > 0) CK(step_set_smem(e.opt.accumulate, smem));
     int bps = 0;
     CK(step_occupancy(e.block, e.opt.accumulate, &bps, smem));
@@ -2065,7 +2065,6 @@ int bsim_autotune(bsim_engine *eh, int32_t trial_steps, bsim_tune_result *out)
     if (e.a.row_off) modes.push_back(BSIM_DELIVERY_PUSH);
     if (e.a.n_tiles > 0) modes.push_back(BSIM_DELIVERY_TILE);
     const int saved_block = e.block, saved_grid = e.grid, saved_del = e.a.delivery;
-    const size_t smem = step_dynamic_smem(e.a);
     cudaEvent_t ev0, ev1;
     CK(cudaEventCreate(&ev0));
     CK(cudaEventCreate(&ev1));
@@ -2078,6 +2077,8 @@ int bsim_autotune(bsim_engine *eh, int32_t trial_steps, bsim_tune_result *out)
     for (int m : modes)
         for (int b : blocks) {
             int bps = 0;
+            const size_t smem = step_dynamic_smem(e.a, b);
+            if (smem > 0) CK(step_set_smem(e.opt.accumulate, smem));
             if (step_occupancy(b, e.opt.accumulate, &bps, smem) != cudaSuccess || bps < 1) continue;
             const int grids[2] = {e.sm_count * bps, e.sm_count};
             for (int g : grids) cands.push_back(Cand{m, b, g, 0.0f, 0ull});

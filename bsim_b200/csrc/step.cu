@@ -888,7 +888,7 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const __grid
         ev = push_phase(a, t, p ^ 1, s_cum, s_seg);
     } else if (tiled) {
         long long *starts = reinterpret_cast<long long *>(s_dyn + 2 * a.tile_max);
-        int *cums = reinterpret_cast<int *>(starts + MAX_WARPS * TILE_SEGS);
+        int *cums = reinterpret_cast<int *>(starts + (blockDim.x >> 5) * TILE_SEGS);
         ev = tile_phase(a, t, p ^ 1, reinterpret_cast<unsigned *>(s_dyn), starts, cums, s_part);
     } else {
         ev = pull_phase<ACC>(a, t, p ^ 1);
@@ -958,10 +958,10 @@ __global__ void record_flush_kernel(const StepArgs a)
 
 // Dynamic shared memory of the step kernel: the tile accumulators and the
 // per-warp segment lists of tiled delivery (0 when no tiles are built).
-size_t step_dynamic_smem(const StepArgs &a)
+size_t step_dynamic_smem(const StepArgs &a, int block)
 {
     if (a.n_tiles == 0) return 0;
-    return (size_t)4 * a.tile_max * sizeof(unsigned) + (size_t)MAX_WARPS * TILE_SEGS * (sizeof(long long) + sizeof(int));
+    return (size_t)4 * a.tile_max * sizeof(unsigned) + (size_t)(block / 32) * TILE_SEGS * (sizeof(long long) + sizeof(int));
 }
 
 // The attribute belongs to the kernel, not to an engine: it only ever grows,
@@ -986,7 +986,7 @@ cudaError_t step_set_smem(int accumulate, size_t bytes)
 
 cudaError_t launch_step(Engine &e)
 {
-    const size_t smem = step_dynamic_smem(e.a);
+    const size_t smem = step_dynamic_smem(e.a, e.block);
     if (e.opt.accumulate == BSIM_ACC_ORDERED)
         step_kernel<BSIM_ACC_ORDERED><<<e.grid, e.block, smem, e.stream>>>(e.a);
     else
