@@ -30,25 +30,53 @@ int fail(int code, const std::string &m, cudaError_t st = cudaSuccess)
     return record_error(code, st == cudaSuccess ? m : m + ": " + cudaGetErrorString(st));
 }
 
-// Thread per sample, parameters staged in shared memory. mode 0: forward only
-// (y_out); mode 1: forward + backward, gradients of the mean loss accumulated
-// with atomics into grad, per-block loss partial into loss_acc.
-template <int MODE>
-__global__ void mlp_kernel(const float *params, const float *x, const float *y_target, int64_t n, float *y_out,
-                           float *grad, double *loss_acc)
+// Forward pass: thread per sample, parameters staged in shared memory.
+__global__ void mlp_forward_kernel(const float *params, const float *x, int64_t n, float *y_out)
 {
     __shared__ float P[NP];
-    __shared__ float G[NP];
-    __shared__ double s_loss;
-    for (int i = threadIdx.x; i < NP; i += blockDim.x) {
-        P[i] = params[i];
-        if (MODE == 1) G[i] = 0.0f;
-    }
-    if (threadIdx.x == 0) s_loss = 0.0;
+    for (int i = threadIdx.x; i < NP; i += blockDim.x) P[i] = params[i];
     __syncthreads();
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float xi[IN], h1[H];
+    for (int k = 0; k < IN; k++) xi[k] = x[i * IN + k];
+    for (int u = 0; u < H; u++) {
+        float s = P[OFF_B1 + u];
+        for (int k = 0; k < IN; k++) s = fmaf(P[OFF_W1 + u * IN + k], xi[k], s);
+        h1[u] = fmaxf(s, 0.0f);
+    }
+    float y = P[OFF_B3];
+    for (int u = 0; u < H; u++) {
+        float s = P[OFF_B2 + u];
+        for (int k = 0; k < H; k++) s = fmaf(P[OFF_W2 + u * H + k], h1[k], s);
+        y = fmaf(P[OFF_W3 + u], fmaxf(s, 0.0f), y);
+    }
+    y_out[i] = y;
+}
+
+// Backward pass over tiles of GT samples, one thread per sample for the
+// forward and the per-sample error terms (kept in shared memory, rows padded to
+// 65 words against bank conflicts), then one thread per group of parameters
+// summing its gradient over the tile's samples: one global atomic per parameter
+// and tile instead of one shared atomic per parameter and sample.
+constexpr int GT = 64, RS = H + 1;
+constexpr size_t GRAD_SMEM = sizeof(float) * (NP + 4 * GT * RS + GT * IN + GT);
+
+__global__ void __launch_bounds__(GT) mlp_grad_kernel(const float *params, const float *x, const float *y_target,
+                                                       int64_t n, float *grad, double *loss_acc)
+{
+    extern __shared__ float sm[];
+    float *P = sm;
+    float *s_h1 = P + NP, *s_h2 = s_h1 + GT * RS, *s_dz2 = s_h2 + GT * RS, *s_dz1 = s_dz2 + GT * RS;
+    float *s_x = s_dz1 + GT * RS, *s_dy = s_x + GT * IN;
+    for (int i = threadIdx.x; i < NP; i += blockDim.x) P[i] = params[i];
+    __syncthreads();
+    const int t = threadIdx.x;
+    const int64_t i = (int64_t)blockIdx.x * GT + t;
+    float *h1 = s_h1 + t * RS, *h2 = s_h2 + t * RS, *dz2 = s_dz2 + t * RS, *dz1 = s_dz1 + t * RS;
+    float *xi = s_x + t * IN;
+    double sq = 0.0;
     if (i < n) {
-        float xi[IN], h1[H], h2[H];
         for (int k = 0; k < IN; k++) xi[k] = x[i * IN + k];
         for (int u = 0; u < H; u++) {
             float s = P[OFF_B1 + u];
@@ -62,41 +90,58 @@ __global__ void mlp_kernel(const float *params, const float *x, const float *y_t
             h2[u] = fmaxf(s, 0.0f);
             y = fmaf(P[OFF_W3 + u], h2[u], y);
         }
-        if (MODE == 0) {
-            y_out[i] = y;
-        } else {
-            const float e = y - y_target[i];
-            atomicAdd(&s_loss, (double)e * (double)e / (double)n);
-            const float dy = 2.0f * e / (float)n;
-            atomicAdd(&G[OFF_B3], dy);
-            float dh1[H];
-            for (int k = 0; k < H; k++) dh1[k] = 0.0f;
-            for (int u = 0; u < H; u++) {
-                atomicAdd(&G[OFF_W3 + u], dy * h2[u]);
-                const float dz2 = h2[u] > 0.0f ? dy * P[OFF_W3 + u] : 0.0f;
-                if (dz2 != 0.0f) {
-                    atomicAdd(&G[OFF_B2 + u], dz2);
-                    for (int k = 0; k < H; k++) {
-                        atomicAdd(&G[OFF_W2 + u * H + k], dz2 * h1[k]);
-                        dh1[k] = fmaf(dz2, P[OFF_W2 + u * H + k], dh1[k]);
-                    }
-                }
-            }
-            for (int u = 0; u < H; u++) {
-                const float dz1 = h1[u] > 0.0f ? dh1[u] : 0.0f;
-                if (dz1 != 0.0f) {
-                    atomicAdd(&G[OFF_B1 + u], dz1);
-                    for (int k = 0; k < IN; k++) atomicAdd(&G[OFF_W1 + u * IN + k], dz1 * xi[k]);
-                }
-            }
+        const float e = y - y_target[i];
+        sq = (double)e * (double)e;
+        const float dy = 2.0f * e / (float)n;
+        s_dy[t] = dy;
+        for (int u = 0; u < H; u++) dz2[u] = h2[u] > 0.0f ? dy * P[OFF_W3 + u] : 0.0f;
+        for (int k = 0; k < H; k++) {
+            float d = 0.0f;
+            for (int u = 0; u < H; u++) d = fmaf(dz2[u], P[OFF_W2 + u * H + k], d);
+            dz1[k] = h1[k] > 0.0f ? d : 0.0f;
         }
+    } else {  // samples past the end contribute nothing
+        s_dy[t] = 0.0f;
+        for (int k = 0; k < IN; k++) xi[k] = 0.0f;
+        for (int u = 0; u < H; u++) h1[u] = h2[u] = dz2[u] = dz1[u] = 0.0f;
     }
-    if (MODE == 1) {
-        __syncthreads();
-        for (int j = threadIdx.x; j < NP; j += blockDim.x)
-            if (G[j] != 0.0f) atomicAdd(&grad[j], G[j]);
-        if (threadIdx.x == 0) atomicAdd(loss_acc, s_loss);
+    for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+    if ((t & 31) == 0 && sq != 0.0) atomicAdd(loss_acc, sq / (double)n);
+    __syncthreads();
+    // gradients of this tile, parameter by parameter
+    for (int j = t; j < NP; j += GT) {
+        float g = 0.0f;
+        if (j < OFF_B1) {  // W1[u][k]
+            const int u = j / IN, k = j % IN;
+            for (int b = 0; b < GT; b++) g = fmaf(s_dz1[b * RS + u], s_x[b * IN + k], g);
+        } else if (j < OFF_W2) {  // b1[u]
+            for (int b = 0; b < GT; b++) g += s_dz1[b * RS + (j - OFF_B1)];
+        } else if (j < OFF_B2) {  // W2[u][k]
+            const int u = (j - OFF_W2) / H, k = (j - OFF_W2) % H;
+            for (int b = 0; b < GT; b++) g = fmaf(s_dz2[b * RS + u], s_h1[b * RS + k], g);
+        } else if (j < OFF_W3) {  // b2[u]
+            for (int b = 0; b < GT; b++) g += s_dz2[b * RS + (j - OFF_B2)];
+        } else if (j < OFF_B3) {  // W3[u]
+            for (int b = 0; b < GT; b++) g = fmaf(s_dy[b], s_h2[b * RS + (j - OFF_W3)], g);
+        } else {  // b3
+            for (int b = 0; b < GT; b++) g += s_dy[b];
+        }
+        if (g != 0.0f) atomicAdd(&grad[j], g);
     }
+}
+
+// Launches the backward pass (the shared-memory size needs the opt-in once).
+cudaError_t launch_grad(const float *p, const float *x, const float *y, int64_t n, float *g, double *l)
+{
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t st = cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)GRAD_SMEM);
+        if (st != cudaSuccess) return st;
+        attr_set = true;
+    }
+    mlp_grad_kernel<<<(unsigned)((n + GT - 1) / GT), GT, GRAD_SMEM>>>(p, x, y, n, g, l);
+    return cudaGetLastError();
 }
 
 __global__ void adam_kernel(float *p, const float *g, float *m, float *v, float lr, float b1t, float b2t)
@@ -165,7 +210,7 @@ extern "C" int bsim_mlp_forward(const float *params, const float *x, int64_t n, 
         return fail(BSIM_ERR_NOMEM, "bsim_mlp_forward: allocation", st);
     cudaMemcpy(dp, params, sizeof(float) * NP, cudaMemcpyHostToDevice);
     cudaMemcpy(dx, x, sizeof(float) * n * IN, cudaMemcpyHostToDevice);
-    mlp_kernel<0><<<(unsigned)((n + 127) / 128), 128>>>(dp, dx, nullptr, n, dy, nullptr, nullptr);
+    mlp_forward_kernel<<<(unsigned)((n + 127) / 128), 128>>>(dp, dx, n, dy);
     st = cudaMemcpy(y, dy, sizeof(float) * n, cudaMemcpyDeviceToHost);
     if (st != cudaSuccess) return fail(BSIM_ERR_CUDA, "bsim_mlp_forward", st);
     return BSIM_OK;
@@ -187,7 +232,7 @@ extern "C" int bsim_mlp_grad(const float *params, const float *x, const float *y
     cudaMemcpy(dt, y_target, sizeof(float) * n, cudaMemcpyHostToDevice);
     cudaMemset(dg, 0, sizeof(float) * NP);
     cudaMemset(dl, 0, sizeof(double));
-    mlp_kernel<1><<<(unsigned)((n + 127) / 128), 128>>>(dp, dx, dt, n, nullptr, dg, dl);
+    if ((st = launch_grad(dp, dx, dt, n, dg, dl)) != cudaSuccess) return fail(BSIM_ERR_CUDA, "bsim_mlp_grad", st);
     double l = 0;
     st = cudaMemcpy(grad, dg, sizeof(float) * NP, cudaMemcpyDeviceToHost);
     if (st == cudaSuccess) st = cudaMemcpy(&l, dl, sizeof(double), cudaMemcpyDeviceToHost);
@@ -231,7 +276,7 @@ extern "C" int bsim_mlp_train(float *params, const float *x, const float *y_targ
             gather_rows<<<64, 256>>>(dx, dt, didx + b0, bs, xb, yb);
             cudaMemsetAsync(dg, 0, sizeof(float) * NP);
             cudaMemsetAsync(dl, 0, sizeof(double));
-            mlp_kernel<1><<<(unsigned)((bs + 127) / 128), 128>>>(dp, xb, yb, bs, nullptr, dg, dl);
+            if ((st = launch_grad(dp, xb, yb, bs, dg, dl)) != cudaSuccess) return fail(BSIM_ERR_CUDA, "bsim_mlp_train", st);
             step++;
             b1t *= 0.9f;
             b2t *= 0.999f;
@@ -241,7 +286,7 @@ extern "C" int bsim_mlp_train(float *params, const float *x, const float *y_targ
     // loss over the whole set
     cudaMemset(dg, 0, sizeof(float) * NP);
     cudaMemset(dl, 0, sizeof(double));
-    mlp_kernel<1><<<(unsigned)((n + 127) / 128), 128>>>(dp, dx, dt, n, nullptr, dg, dl);
+    if ((st = launch_grad(dp, dx, dt, n, dg, dl)) != cudaSuccess) return fail(BSIM_ERR_CUDA, "bsim_mlp_train", st);
     double l = 0;
     st = cudaMemcpy(params, dp, sizeof(float) * NP, cudaMemcpyDeviceToHost);
     if (st == cudaSuccess) st = cudaMemcpy(&l, dl, sizeof(double), cudaMemcpyDeviceToHost);
