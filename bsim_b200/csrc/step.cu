@@ -274,15 +274,22 @@ static __device__ __forceinline__ unsigned long long push_phase(const StepArgs &
     unsigned long long ev = 0;
     unsigned long long *acc = reinterpret_cast<unsigned long long *>(a.acc) + 2 * (int64_t)pw * a.n_planes * a.N;
     const long long n_warps = ((long long)gridDim.x * blockDim.x) >> 5;
-    const long long n_chunks = (total + PUSH_CHUNK - 1) / PUSH_CHUNK;
-    for (long long ch = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; ch < n_chunks; ch += n_warps) {
+    // Segments per warp chunk: PUSH_CHUNK when there are enough for every warp, fewer
+    // (down to one) when a cycle has few spikes with long rows, so that more warps
+    // share the rows. Chunks go to warps block-interleaved (chunk c to warp c / grid of
+    // block c % grid), so a cycle with few chunks still spreads over every SM.
+    int pc = PUSH_CHUNK;
+    while (pc > 1 && total < (long long)pc * n_warps) pc >>= 1;
+    const long long n_chunks = (total + pc - 1) / pc;
+    const long long warp_lin = (long long)(threadIdx.x >> 5) * gridDim.x + blockIdx.x;
+    for (long long ch = warp_lin; ch < n_chunks; ch += n_warps) {
         // Lanes 0..PUSH_CHUNK-1 each resolve one (spike, delay) segment: its row
         // [r0, r1), split into an odd head entry, 16-byte pairs [p0, p0 + 2*np)
         // and an odd tail entry.
         int64_t r0 = 0, r1 = 0;
         float sc = 0.0f;
-        const long long item = ch * PUSH_CHUNK + lane;
-        if (lane < PUSH_CHUNK && item < total) {
+        const long long item = ch * pc + lane;
+        if (lane < pc && item < total) {
             int lo = 1, hi = D;
             while (lo < hi) {
                 const int mid = (lo + hi) >> 1;
@@ -336,14 +343,19 @@ static __device__ __forceinline__ unsigned long long push_phase(const StepArgs &
             }
         }
         // the pairs of all segments as one flat range, four loads in flight per lane
+        // each chunk walks its range from its own starting point (wrapping around), so that
+        // chunks whose rows hit the same targets (a population's sources in a dense
+        // projection) do not add into the same addresses in lockstep
+        const long long rot = total_pairs > 0 ? (long long)((unsigned long long)(ch * 40503ll) % total_pairs) : 0;
         for (long long pb = 0; pb < total_pairs; pb += 4 * 32) {
             uint4 x[4];
             float xs[4];
             bool ok[4];
 #pragma unroll
             for (int u = 0; u < 4; u++) {
-                const long long p = pb + u * 32 + lane;
-                ok[u] = p < total_pairs;
+                const long long q = pb + u * 32 + lane;
+                ok[u] = q < total_pairs;
+                const long long p = q + rot < total_pairs ? q + rot : q + rot - total_pairs;
                 int k = 0;
                 while (k < PUSH_CHUNK - 1 && p >= seg[k].incl) k++;
                 const long long excl = k == 0 ? 0 : seg[k - 1].incl;
