@@ -241,6 +241,7 @@ class Engine:
 
     def __init__(self, handle):
         self._h = handle
+        self._rec_steps = None  # steps of the current recording (sizes the offsets read back)
 
     @classmethod
     def from_arrays(cls, params, src, dst, weight, delay_steps, dt, pop=None, instance=None, opts=None,
@@ -288,15 +289,22 @@ class Engine:
 
     def record(self, max_steps, capacity):
         _check(lib().bsim_record(self._h, max_steps, capacity))
+        self._rec_steps = max_steps
 
     def raster(self, out=None):
         """Recorded spikes: list of int32 arrays (ascending ids), one per recorded step.
         The arrays are views into one buffer read in a single copy from the device:
         `out` (a C-contiguous int32 array, e.g. in page-locked memory, reused across
         reads) when it is large enough, else a new array."""
-        info = self.info()
-        off = np.zeros(info.steps_done + 2, np.int64)
+        if self._rec_steps is None:
+            self._rec_steps = self.info().steps_done + 1
+        off = np.zeros(self._rec_steps + 2, np.int64)
         ns = ctypes.c_int64()
+        if out is not None and out.dtype == np.int32 and out.ndim == 1 and out.flags.c_contiguous:
+            # one call: sizes and ids together when `out` is large enough
+            rc = lib().bsim_read_raster(self._h, _p(off), _p(out), out.shape[0], ctypes.byref(ns))
+            if rc == BSIM_OK:
+                return [out[off[k]:off[k + 1]] for k in range(ns.value)]
         _check(lib().bsim_read_raster(self._h, _p(off), None, 0, ctypes.byref(ns)))
         total = int(off[ns.value])
         if (out is not None and out.dtype == np.int32 and out.ndim == 1 and out.flags.c_contiguous
