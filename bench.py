@@ -651,6 +651,14 @@ def main():
         cnt_buf = np.empty(N, np.int32)
     eng.record(e2e_steps, cap)  # allocates the recording buffers (drops the captured graph)
     eng.run(100)                # re-captures the graph with recording enabled (not timed)
+    # one untimed pass of the whole path first, so that the timed one does not pay for
+    # loading the kernels it launches for the first time (the state packing, the raster's
+    # flush and sort)
+    eng.record(e2e_steps, cap)
+    eng.write_state(v, ie, ii, rf)
+    eng.run(e2e_steps)
+    eng.raster(out=ras_buf)
+    eng.fire_count(out=cnt_buf)
     eng.record(e2e_steps, cap)  # re-arms the recording only
     if dist:
         dist.barrier()

@@ -603,28 +603,14 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
                 const int excl = incl - cnt;
                 const int total = __shfl_sync(0xffffffffu, incl, 31);
                 const int take = max(0, min(cnt, TILE_SEGS - excl));
-                // the lane's fired segments, four at a time: their offset loads are all
-                // issued before any is used, so a lane with several fired sources waits
-                // about one load latency per four segments, not one per segment
-                for (int i0 = 0; i0 < take; i0 += 4) {
-                    uint2 sg[4];
-#pragma unroll
-                    for (int u = 0; u < 4; u++) {
-                        if (i0 + u < take) {
-                            const int b = __ffs(m) - 1;
-                            m &= m - 1;
-                            // in 16-byte units: segments start on an even entry and have even length
-                            const uint32_t *ps = a.pair_seg + (kbase + b) * (D + 1) + (d - 1);
-                            sg[u] = make_uint2(ps[0], ps[1]);
-                        }
-                    }
-#pragma unroll
-                    for (int u = 0; u < 4; u++) {
-                        if (i0 + u < take) {
-                            seg_start[excl + i0 + u] = seg0 + (long long)sg[u].x;
-                            seg_cum[excl + i0 + u] = (int)(sg[u].y - sg[u].x);  // length for now
-                        }
-                    }
+                for (int i = 0; i < take; i++) {
+                    const int b = __ffs(m) - 1;
+                    m &= m - 1;
+                    // in 16-byte units: segments start on an even entry and have even length
+                    const uint32_t *ps = a.pair_seg + (kbase + b) * (D + 1) + (d - 1);
+                    const uint32_t s0 = ps[0], s1 = ps[1];
+                    seg_start[excl + i] = seg0 + (long long)s0;
+                    seg_cum[excl + i] = (int)(s1 - s0);  // length for now
                 }
                 __syncwarp();
                 const int nseg = min(total, TILE_SEGS);

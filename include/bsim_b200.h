@@ -79,7 +79,8 @@ typedef struct bsim_options {
     int32_t tile_size;     /* target neurons per tile (0: chosen from the network size and delays, <= 5000) */
     int32_t lif_blocks;    /* blocks of the step kernel that run the neuron update (the others start
                               delivering at once; both halves of a cycle touch disjoint data, so the
-                              bandwidth-bound update overlaps the delivery); 0: every block */
+                              bandwidth-bound update overlaps the delivery); 0: one per SM with
+                              tiled delivery, every block otherwise */
     int32_t reserved[6];
 } bsim_options;
 

@@ -148,7 +148,7 @@ def test_noalloc_flags_corrupt_inputs_without_running_them():
             k = int(torch.nonzero(b["row_off"][1:] > b["row_off"][:-1])[5])
             b["row_off"][k + 1] = b["row_off"][k] - 1
         elif what == "rows_end":
-            b["row_off"][-1] -= 2
+            b["row_off"][-1] += 2  # still ascending, but past the synapse count
         elif what == "class":
             b["cls"][7] = 4  # 4 classes (one per population): 4 is past the table
         elif what == "kind":
