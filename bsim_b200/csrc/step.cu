@@ -463,7 +463,10 @@ static __device__ __forceinline__ unsigned long long pull_phase(const StepArgs &
 // every carry is counted once); the fixed-point exponent keeps every sum below
 // 2^61, so the high word cannot overflow.
 // ---------------------------------------------------------------------------
-#define TILE_SEGS 64
+#ifndef TILE_SEGS
+#define TILE_SEGS 64  // fired segments a warp lists per round
+#endif
+static_assert(TILE_SEGS >= 32 && TILE_SEGS <= 64, "a round's segment prefix covers two entries per lane");
 #ifndef TILE_CHUNK_PAIRS
 #define TILE_CHUNK_PAIRS 512  // entry pairs a chunk of units should list (from the previous cycle's rate)
 #endif
