@@ -40,7 +40,7 @@ class Options(ctypes.Structure):
                 ("build_pull", ctypes.c_int32), ("graph_steps", ctypes.c_int32),
                 ("block_threads", ctypes.c_int32), ("grid_blocks", ctypes.c_int32),
                 ("build_tiles", ctypes.c_int32), ("tile_size", ctypes.c_int32),
-                ("lif_blocks", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6)]
+                ("reserved", ctypes.c_int32 * 7)]
 
 
 class GenSpec(ctypes.Structure):

@@ -530,10 +530,6 @@ static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
     a.delivery = (e.opt.delivery == BSIM_DELIVERY_PULL || e.opt.delivery == BSIM_DELIVERY_AUTO) ? e.opt.delivery
                                                                                                  : BSIM_DELIVERY_PUSH;
     a.deliv_sel = nullptr;
-    // Tiled delivery: one neuron-update block per SM by default; the other blocks start
-    // delivering at once (measured ~1 % faster on the 1e6-neuron network than every block
-    // updating first, and slower with fewer update blocks).
-    a.lif_blocks = e.opt.lif_blocks;
     a.rec_ids = nullptr;
     a.rec_off = nullptr;
     a.rec = nullptr;
@@ -541,7 +537,6 @@ static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
     a.n_pops = e.n_pops;
     a.hist_len = 0;
     if (a.n_tiles > 0 && e.opt.delivery == BSIM_DELIVERY_TILE) a.delivery = BSIM_DELIVERY_TILE;
-    if (a.lif_blocks == 0 && a.delivery == BSIM_DELIVERY_TILE) a.lif_blocks = e.sm_count;
     // every cycle of a tiled-only engine overwrites all planes of the parity it
     // delivers into, so the LIF phase need not clear them; any other mode adds
     a.acc_clear = a.delivery == BSIM_DELIVERY_TILE ? 0 : 1;

@@ -92,7 +92,6 @@ struct StepArgs {
     int32_t *err;                  // device error flag (0 = ok)
     const int32_t *deliv_sel;      // per-step delivery choice written by the predictor (may be NULL)
     int32_t delivery;              // BSIM_DELIVERY_PUSH / _PULL when deliv_sel is NULL
-    int32_t lif_blocks;            // blocks [0, lif_blocks) run the neuron update (grid-stride over them)
     // raster recording (control words in device memory so a captured graph stays valid)
     int32_t *rec_ids;           // [rec->cap]
     int64_t *rec_off;           // [rec->steps + 1]

@@ -1,11 +1,13 @@
 // The fused simulation step for sm_100a.
 //
 // One launch advances every network in the engine by one cycle. Its blocks
-// first run the LIF_brian update over a grid-stride share of the neurons
-// (reads the synaptic input summed during the previous launch, writes the new
-// state, appends fired ids to this cycle's ring slot with one atomic per block
-// pass and stores each warp's ballot as a fired-bitmap word), then deliver the
-// spikes of cycles t-1 .. t-D into the input buffer of cycle t+1.
+// first deliver the spikes of cycles t-1 .. t-D into the input buffer of cycle
+// t+1, then run the LIF_brian update of cycle t in chunks of neurons taken from
+// a per-cycle counter (reads the synaptic input summed during the previous
+// launch, writes the new state, appends fired ids to this cycle's ring slot with
+// one atomic per block pass and stores each warp's ballot as a fired-bitmap
+// word). Blocks that finish delivering early take most of the update, so the
+// bandwidth-bound update fills the tail of the delivery.
 //
 // The two halves touch disjoint data (the input accumulators are double
 // buffered by cycle parity, the fire ring has D+2 slots), so they need no
@@ -84,9 +86,9 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
                                                  int *s_wcnt)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const int nb = (a.lif_blocks > 0 && a.lif_blocks < (int)gridDim.x) ? a.lif_blocks : (int)gridDim.x;
-    if ((int)blockIdx.x >= nb) return;  // this block starts delivering at once
-    const int64_t stride = (int64_t)nb * blockDim.x;
+    // the cycle's chunk counter: the upper half of the ticket word (reset by the last block)
+    unsigned *chunk_ctr = a.ticket + 1;
+    __shared__ long long s_chunk;
     int32_t *slot_ids = a.ring + (int64_t)cur * a.cap;
     uint32_t *bm = a.bitmap + (int64_t)cur * a.W;
     int32_t *hist = a.pop_hist ? a.pop_hist + (int64_t)(t % (unsigned long long)a.hist_len) * a.n_pops : nullptr;
@@ -104,7 +106,14 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
         }
     }
     int buf = 0;  // s_wcnt is double-buffered by pass, so a pass needs no closing barrier
-    for (int64_t bbase = (int64_t)blockIdx.x * blockDim.x; bbase < a.N; bbase += stride, buf ^= 64) {
+    for (;;) {
+        // one pass of blockDim.x neurons per chunk
+        if (threadIdx.x == 0) s_chunk = (long long)atomicAdd(chunk_ctr, (unsigned)blockDim.x);
+        __syncthreads();
+        const int64_t bbase = s_chunk;
+        __syncthreads();
+        if (bbase >= a.N) break;
+        buf ^= 64;
         const int64_t base = bbase + (threadIdx.x & ~31);
         const int64_t j = base + lane;
         bool fired = false;
@@ -204,9 +213,8 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
             }
         }
         // no barrier here: the next pass writes the other half of s_wcnt, and the pass
-        // after it is ordered by the next pass's two barriers
+        // after it is ordered by the next pass's barriers
     }
-    __syncthreads();  // s_wcnt is free for the caller
 }
 
 // ---------------------------------------------------------------------------
@@ -881,7 +889,6 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const __grid
         int32_t *nxt = a.pop_hist + (int64_t)((t + 1) % (unsigned long long)a.hist_len) * a.n_pops;
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_pops; i += gridDim.x * blockDim.x) nxt[i] = 0;
     }
-    lif_phase<ACC>(a, t, p, cur, s_wcnt);
     record_phase(a, t);
     __syncthreads();  // publishes s_cum and s_ev
     unsigned long long ev;
@@ -895,6 +902,7 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const __grid
         ev = pull_phase<ACC>(a, t, p ^ 1);
     }
     if (ev) atomicAdd(&s_ev, ev);
+    lif_phase<ACC>(a, t, p, cur, s_wcnt);
     if (a.mlp && a.pop_hist) predict_phase(a, t);
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -926,6 +934,7 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const __grid
                 }
             }
             *a.ticket = 0u;
+            *(a.ticket + 1) = 0u;  // the update's chunk counter
             if (a.part_ctr) *a.part_ctr = 0u;
             *a.step_ctr = t + 1;
             __threadfence();

@@ -77,11 +77,7 @@ typedef struct bsim_options {
     int32_t build_tiles;   /* 1: also build the target-tiled copy; 0: only for TILE/AUTO; -1: never
                               (an AUTO engine then pushes every cycle; saves ~8 B per synapse) */
     int32_t tile_size;     /* target neurons per tile (0: chosen from the network size and delays, <= 5000) */
-    int32_t lif_blocks;    /* blocks of the step kernel that run the neuron update (the others start
-                              delivering at once; both halves of a cycle touch disjoint data, so the
-                              bandwidth-bound update overlaps the delivery); 0: one per SM with
-                              tiled delivery, every block otherwise */
-    int32_t reserved[6];
+    int32_t reserved[7];
 } bsim_options;
 
 /* Parameters of one generated network (see bsim_create_generated). */
