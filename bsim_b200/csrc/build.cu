@@ -432,7 +432,7 @@ static int create_from_arrays(const float *params, const uint8_t *kind, int64_t 
 }
 
 #ifndef MAX_PLANES
-#define MAX_PLANES 8  // parts per tile (accumulator planes)
+#define MAX_PLANES 8  // parts per tile
 #endif
 #ifndef MIN_PLANES
 #define MIN_PLANES 1  // parts per tile at least (blocks that run out of parts help the others)
@@ -451,21 +451,24 @@ static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
     TRY(dalloc(e, &d_ctab, ctab.size()));
     CK(cudaMemcpy(d_ctab, ctab.data(), sizeof(ClassParams) * ctab.size(), cudaMemcpyHostToDevice));
     a.ctab = d_ctab;
-    // tiled delivery: each tile's work units in P parts, one accumulator plane per
-    // part plus the help plane; about two parts per resident block (occupancy 2
-    // blocks/SM), at least MIN_PLANES
+    // tiled delivery: each tile's work units in P parts, about two parts per resident
+    // block (occupancy 2 blocks/SM), at least MIN_PLANES; all parts of a tile (and the
+    // blocks helping them) sum into one accumulator plane: the first to finish stores
+    // its sums, the others add theirs once that store is done
     a.n_planes = 1;
     a.n_parts = 0;
     a.parts = nullptr;
     a.part_next = nullptr;
     a.part_pairs = nullptr;
-    a.help_plane = -1;
+    a.tile_arrive = nullptr;
     if (a.n_tiles > 0) {
         const int nt = a.n_tiles;
         const double want = 4.0 * e.sm_count / nt;
         const int P = (int)std::max((double)MIN_PLANES, std::min((double)MAX_PLANES, std::floor(want + 0.5)));
-        a.n_planes = P + 1;  // the parts' planes and the help plane
-        a.help_plane = P;
+        unsigned int *d_arrive;
+        TRY(dalloc(e, &d_arrive, 2 * (size_t)nt));  // [2][n_tiles]: finishers so far, first store done
+        CK(cudaMemset(d_arrive, 0, sizeof(unsigned int) * 2 * nt));
+        a.tile_arrive = d_arrive;
         std::vector<int4> parts;
         for (int q = 0; q < nt; q++) {
             const int U = q < (int)e.tile_units.size() ? e.tile_units[q] : 0;

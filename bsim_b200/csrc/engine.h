@@ -105,10 +105,10 @@ struct StepArgs {
     // target-tiled delivery (BSIM_DELIVERY_TILE). A tile is a target range whose
     // excitatory and inhibitory sums are formed in shared memory. Its sources form
     // runs of consecutive neuron ids; every source of a run owns one (tile, source)
-    // pair. A tile's work units are split into n_planes parts, handed to blocks by a
-    // per-cycle queue; part k stores its sums into accumulator plane k. A block that
-    // finds the queue empty joins the part with the most units left and adds its sums
-    // into the help plane (reduction atomics; the LIF phase reads and clears it).
+    // pair. A tile's work units are split into parts, handed to blocks by a per-cycle
+    // queue. A block that finds the queue empty joins the part with the most units
+    // left. Every block that worked on a tile stores (the first to finish) or adds (the
+    // others, once that store is done) its sums into the one accumulator plane.
     int32_t n_tiles;                 // tiles (0: no tiled copy)
     int32_t n_tiles_u;               // = n_tiles (target ranges)
     int32_t n_parts;                 // = n_tiles * n_planes
@@ -119,7 +119,9 @@ struct StepArgs {
                                      // of any part (reset to the first unit by the last block)
     unsigned int *part_pairs;        // [2][n_parts] entry pairs listed per part, by cycle parity;
                                      // the previous cycle's count sizes the part's chunks
-    int32_t help_plane;              // plane blocks that join another block's part add into (-1: none)
+    unsigned int *tile_arrive;       // [2][n_tiles]: blocks that finished a piece of the tile this
+                                     // cycle, and whether the first one's store is done (reset by
+                                     // the last block)
     int32_t tile_max;                // largest range (neurons): shared-memory accumulator size
     const int32_t *tile_beg;         // [n_tiles + 1] first target of each tile
     const float *tile_scale;         // [n_tiles] 2^qexp of the tile's network

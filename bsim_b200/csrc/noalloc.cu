@@ -172,7 +172,6 @@ extern "C" int bsim_run_noalloc(int64_t n, int32_t max_delay, void *state_dev, c
     a.n_pops = 1;
     a.n_planes = 1;
     a.acc_clear = 1;
-    a.help_plane = -1;
 
     // The previous call's contents are still in the array: clear what must
     // start at zero (input accumulators of both parities, ring counts, bitmaps,

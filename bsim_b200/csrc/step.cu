@@ -134,8 +134,6 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
                 }
                 if (a.acc_clear)
                     for (int k = 0; k < a.n_planes; k++) acc[(int64_t)k * a.N] = make_longlong2(0, 0);
-                else if (a.help_plane >= 0)
-                    acc[(int64_t)a.help_plane * a.N] = make_longlong2(0, 0);
                 const float sd = __ldg(&c->scale_down);
                 inE = __fmul_rn(__ll2float_rn(q.x), sd);
                 inI = __fmul_rn(__ll2float_rn(q.y), sd);
@@ -471,6 +469,9 @@ static __device__ __forceinline__ unsigned long long pull_phase(const StepArgs &
 // every carry is counted once); the fixed-point exponent keeps every sum below
 // 2^61, so the high word cannot overflow.
 // ---------------------------------------------------------------------------
+#ifndef TILE_WAIT_SPINS
+#define TILE_WAIT_SPINS (1u << 22)  // ~0.3 s of 64 ns sleeps: far beyond any store phase
+#endif
 #ifndef TILE_SEGS
 #define TILE_SEGS 64  // fired segments a warp lists per round
 #endif
@@ -688,17 +689,38 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
         }
         if (lane == 0 && listed) atomicAdd(pairs_cnt, listed);
         __syncthreads();
-        if (!helper) {
-            // the owner stores the part's plane of the tile's {E, I} accumulator pairs
-            longlong2 *g = reinterpret_cast<longlong2 *>(a.acc) + ((int64_t)pw * a.n_planes + part.w) * a.N + tb;
+        // Flush into the tile's one accumulator plane. The first block to finish a piece of
+        // the tile this cycle (an owner or a helper) stores its sums; every other block waits
+        // until that store is done and adds its sums with reductions. The first finisher
+        // never waits, so the waits always end; they are bounded all the same.
+        if (threadIdx.x == 0) {
+            const unsigned k = atomicAdd(a.tile_arrive + q, 1u);
+            if (k != 0u) {
+                const volatile unsigned *done = a.tile_arrive + a.n_tiles + q;
+                unsigned spins = 0;
+                while (*done == 0u) {
+                    if (++spins > TILE_WAIT_SPINS) {
+                        raise_error(a, BSIM_DEVERR_TIMEOUT);
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+                __threadfence();
+            }
+            s_part[1] = k == 0u;
+        }
+        __syncthreads();
+        if (s_part[1]) {
+            longlong2 *g = reinterpret_cast<longlong2 *>(a.acc) + (int64_t)pw * a.N + tb;
             for (int i = threadIdx.x; i < T; i += blockDim.x) {
                 g[i] = make_longlong2(carry_sum(s_acc + i, T), carry_sum(s_acc + 2 * T + i, T));
                 s_acc[i] = s_acc[T + i] = s_acc[2 * T + i] = s_acc[3 * T + i] = 0u;
             }
+            __threadfence();
+            __syncthreads();
+            if (threadIdx.x == 0) atomicExch(a.tile_arrive + a.n_tiles + q, 1u);
         } else {
-            // a helper adds what it summed into the help plane
-            unsigned long long *g = reinterpret_cast<unsigned long long *>(a.acc) +
-                                    2 * (((int64_t)pw * a.n_planes + a.help_plane) * a.N + tb);
+            unsigned long long *g = reinterpret_cast<unsigned long long *>(a.acc) + 2 * ((int64_t)pw * a.N + tb);
             for (int i = threadIdx.x; i < T; i += blockDim.x) {
                 const long long e = carry_sum(s_acc + i, T), v = carry_sum(s_acc + 2 * T + i, T);
                 s_acc[i] = s_acc[T + i] = s_acc[2 * T + i] = s_acc[3 * T + i] = 0u;
@@ -912,12 +934,15 @@ __global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const __grid
     }
     __syncthreads();
     if (s_last) {
-        // every other block has finished this cycle: the parts' unit counters start over
-        if (tiled)
+        // every other block has finished this cycle: the parts' unit counters and the
+        // tiles' finisher counts start over
+        if (tiled) {
             for (int i = threadIdx.x; i < a.n_parts; i += blockDim.x) {
                 a.part_next[i] = (unsigned)a.parts[i].y;
                 a.part_help[i] = 0u;
             }
+            for (int i = threadIdx.x; i < 2 * a.n_tiles; i += blockDim.x) a.tile_arrive[i] = 0u;
+        }
         // the next cycle counts its listed pairs from zero (whichever delivery this cycle used)
         if (a.part_pairs)
             for (int i = threadIdx.x; i < a.n_parts; i += blockDim.x)

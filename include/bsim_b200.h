@@ -39,6 +39,7 @@ extern "C" {
 #define BSIM_DEVERR_CLASS 3    /* a class index beyond the class table, or a class of a kind
                                   the entry point does not take */
 #define BSIM_DEVERR_ROWS_END 4 /* row offsets do not start at 0 or do not end at the synapse count */
+#define BSIM_DEVERR_TIMEOUT 5  /* a bounded wait inside the step ran out (the step's result is not trusted) */
 
 #define BSIM_MAX_DELAY 1024    /* delays are 1..BSIM_MAX_DELAY steps */
 #define BSIM_MAX_CLASSES 65535 /* distinct folded LIF parameter tuples per engine */
