@@ -236,7 +236,11 @@ static __device__ __forceinline__ void push_one(const StepArgs &a, unsigned long
 #ifndef PUSH_CHUNK
 #define PUSH_CHUNK 8
 #endif
-// resident blocks of 512 threads the step kernel is compiled for
+// resident blocks of STEP_MAX_THREADS threads the step kernel is compiled for
+// (together they set its register budget: 65,536 / (2 x 512) = 64 per thread)
+#ifndef STEP_MAX_THREADS
+#define STEP_MAX_THREADS 512
+#endif
 #ifndef STEP_MIN_BLOCKS
 #define STEP_MIN_BLOCKS 2
 #endif
@@ -876,7 +880,7 @@ static __device__ __forceinline__ void record_phase(const StepArgs &a, unsigned 
 }
 
 template <int ACC>
-__global__ void __launch_bounds__(512, STEP_MIN_BLOCKS) step_kernel(const __grid_constant__ StepArgs a)
+__global__ void __launch_bounds__(STEP_MAX_THREADS, STEP_MIN_BLOCKS) step_kernel(const __grid_constant__ StepArgs a)
 {
     __shared__ long long s_cum[BSIM_MAX_DELAY + 1];
     __shared__ PushSeg s_seg[MAX_WARPS * PUSH_CHUNK];
