@@ -88,7 +88,7 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     // the cycle's chunk counter: the upper half of the ticket word (reset by the last block)
     unsigned *chunk_ctr = a.ticket + 1;
-    __shared__ long long s_chunk;
+    __shared__ long long s_chunk[2];  // this pass's chunk and the next one's (taken during the pass)
     int32_t *slot_ids = a.ring + (int64_t)cur * a.cap;
     uint32_t *bm = a.bitmap + (int64_t)cur * a.W;
     int32_t *hist = a.pop_hist ? a.pop_hist + (int64_t)(t % (unsigned long long)a.hist_len) * a.n_pops : nullptr;
@@ -106,13 +106,17 @@ static __device__ __forceinline__ void lif_phase(const StepArgs &a, unsigned lon
         }
     }
     int buf = 0;  // s_wcnt is double-buffered by pass, so a pass needs no closing barrier
+    int cb = 0;
+    if (threadIdx.x == 0) s_chunk[0] = (long long)atomicAdd(chunk_ctr, (unsigned)blockDim.x);
+    __syncthreads();
     for (;;) {
-        // one pass of blockDim.x neurons per chunk
-        if (threadIdx.x == 0) s_chunk = (long long)atomicAdd(chunk_ctr, (unsigned)blockDim.x);
-        __syncthreads();
-        const int64_t bbase = s_chunk;
-        __syncthreads();
+        // one pass of blockDim.x neurons per chunk; the next chunk is taken while this one
+        // runs (its slot is read only after this pass's two barriers, and this slot is
+        // written again only in the next pass, after every thread has read it)
+        const int64_t bbase = s_chunk[cb];
         if (bbase >= a.N) break;
+        if (threadIdx.x == 0) s_chunk[cb ^ 1] = (long long)atomicAdd(chunk_ctr, (unsigned)blockDim.x);
+        cb ^= 1;
         buf ^= 64;
         const int64_t base = bbase + (threadIdx.x & ~31);
         const int64_t j = base + lane;
