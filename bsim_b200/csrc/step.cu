@@ -623,14 +623,24 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
                 const int excl = incl - cnt;
                 const int total = __shfl_sync(0xffffffffu, incl, 31);
                 const int take = max(0, min(cnt, TILE_SEGS - excl));
-                for (int i = 0; i < take; i++) {
-                    const int b = __ffs(m) - 1;
+                // the lane's fired segments, two at a time: both offset loads are issued
+                // before either is used (more at once costs registers the streaming loop needs)
+                for (int i = 0; i < take; i += 2) {
+                    const int b0 = __ffs(m) - 1;
                     m &= m - 1;
+                    const bool two = i + 1 < take;
+                    const int b1 = two ? __ffs(m) - 1 : b0;
+                    if (two) m &= m - 1;
                     // in 16-byte units: segments start on an even entry and have even length
-                    const uint32_t *ps = a.pair_seg + (kbase + b) * (D + 1) + (d - 1);
-                    const uint32_t s0 = ps[0], s1 = ps[1];
-                    seg_start[excl + i] = seg0 + (long long)s0;
-                    seg_cum[excl + i] = (int)(s1 - s0);  // length for now
+                    const uint32_t *p0 = a.pair_seg + (kbase + b0) * (D + 1) + (d - 1);
+                    const uint32_t *p1 = a.pair_seg + (kbase + b1) * (D + 1) + (d - 1);
+                    const uint32_t x0 = p0[0], y0 = p0[1], x1 = p1[0], y1 = p1[1];
+                    seg_start[excl + i] = seg0 + (long long)x0;
+                    seg_cum[excl + i] = (int)(y0 - x0);  // length for now
+                    if (two) {
+                        seg_start[excl + i + 1] = seg0 + (long long)x1;
+                        seg_cum[excl + i + 1] = (int)(y1 - x1);
+                    }
                 }
                 __syncwarp();
                 const int nseg = min(total, TILE_SEGS);
