@@ -477,6 +477,9 @@ static __device__ __forceinline__ unsigned long long pull_phase(const StepArgs &
 // every carry is counted once); the fixed-point exponent keeps every sum below
 // 2^61, so the high word cannot overflow.
 // ---------------------------------------------------------------------------
+#ifndef TILE_HELP_MIN
+#define TILE_HELP_MIN 64  // units a part must have left per helping block for another block to join
+#endif
 #ifndef TILE_WAIT_SPINS
 #define TILE_WAIT_SPINS (1u << 22)  // ~0.3 s of 64 ns sleeps: far beyond any store phase
 #endif
@@ -563,7 +566,7 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
             if (lane == 0 && best) atomicMax(s_best, best);
             __syncthreads();
             const unsigned long long b = *s_best;
-            pi = (b >> 32) >= 64ull ? (int)(b & 0xffffffffull) : -1;
+            pi = (b >> 32) >= (unsigned long long)TILE_HELP_MIN ? (int)(b & 0xffffffffull) : -1;
             if (pi >= 0 && threadIdx.x == 0) atomicAdd(a.part_help + pi, 1u);
         }
         __syncthreads();  // every thread has read s_part / s_best before they are written again
