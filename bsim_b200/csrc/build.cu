@@ -434,6 +434,9 @@ static int create_from_arrays(const float *params, const uint8_t *kind, int64_t 
 #ifndef MAX_PLANES
 #define MAX_PLANES 8  // parts per tile
 #endif
+#ifndef TILE_PARTS_PER_SM
+#define TILE_PARTS_PER_SM 4  // parts over all tiles per SM (about two per resident block)
+#endif
 #ifndef MIN_PLANES
 #define MIN_PLANES 1  // parts per tile at least (blocks that run out of parts help the others)
 #endif
@@ -463,7 +466,7 @@ static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
     a.tile_arrive = nullptr;
     if (a.n_tiles > 0) {
         const int nt = a.n_tiles;
-        const double want = 4.0 * e.sm_count / nt;
+        const double want = (double)TILE_PARTS_PER_SM * e.sm_count / nt;
         const int P = (int)std::max((double)MIN_PLANES, std::min((double)MAX_PLANES, std::floor(want + 0.5)));
         unsigned int *d_arrive;
         TRY(dalloc(e, &d_arrive, 2 * (size_t)nt));  // [2][n_tiles]: finishers so far, first store done
