@@ -432,7 +432,7 @@ static int create_from_arrays(const float *params, const uint8_t *kind, int64_t 
 }
 
 #ifndef MAX_PLANES
-#define MAX_PLANES 8  // parts per tile
+#define MAX_PLANES 8  // parts per tile at most
 #endif
 #ifndef TILE_PARTS_PER_SM
 #define TILE_PARTS_PER_SM 3.4  // parts over all tiles per SM, about two per resident block (measured:
@@ -455,10 +455,12 @@ static int finish_engine(Engine &e, const std::vector<ClassParams> &ctab)
     TRY(dalloc(e, &d_ctab, ctab.size()));
     CK(cudaMemcpy(d_ctab, ctab.data(), sizeof(ClassParams) * ctab.size(), cudaMemcpyHostToDevice));
     a.ctab = d_ctab;
-    // tiled delivery: each tile's work units in P parts, about two parts per resident
-    // block (occupancy 2 blocks/SM), at least MIN_PLANES; all parts of a tile (and the
+    // tiled delivery: each tile's work units in P parts (TILE_PARTS_PER_SM parts per SM
+    // over all tiles, MIN_PLANES..MAX_PLANES per tile); all parts of a tile (and the
     // blocks helping them) sum into one accumulator plane: the first to finish stores
-    // its sums, the others add theirs once that store is done
+    // its sums, the others add theirs once that store is done. One plane per parity for
+    // every delivery mode (the step kernel keeps the plane count a runtime value: with
+    // the count folded away its code generation measured 1-15 % slower)
     a.n_planes = 1;
     a.n_parts = 0;
     a.parts = nullptr;

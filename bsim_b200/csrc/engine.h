@@ -74,7 +74,7 @@ struct StepArgs {
     const ClassParams *ctab;   // [n_cls]
     void *acc;                 // [2][n_planes][N] longlong2 (EXACT) or [2][N] float2 (ORDERED): input
                                // for the next step; a target's input is the sum over its planes
-    int32_t n_planes;          // accumulator planes (tiled delivery: one per part of a tile)
+    int32_t n_planes;          // accumulator planes per parity (1 in every configuration)
     int32_t acc_clear;         // the LIF phase zeroes the planes it read (0: every cycle overwrites them)
     uint32_t *bitmap;          // [R][W] fired flags of each step in the ring
     int32_t *ring;             // [R][cap] fired ids of each step in the ring
@@ -111,8 +111,9 @@ struct StepArgs {
     // others, once that store is done) its sums into the one accumulator plane.
     int32_t n_tiles;                 // tiles (0: no tiled copy)
     int32_t n_tiles_u;               // = n_tiles (target ranges)
-    int32_t n_parts;                 // = n_tiles * n_planes
-    const int4 *parts;               // [n_parts] {tile, first unit, end unit, plane}, largest first
+    int32_t n_parts;                 // parts over all tiles
+    const int4 *parts;               // [n_parts] {tile, first unit, end unit, part within the tile},
+                                     // largest first
     unsigned int *part_ctr;          // next part to hand out (reset by the last block of a cycle)
     unsigned int *part_help;         // [n_parts] blocks helping each part this cycle
     unsigned int *part_next;         // [n_parts] next unit of each part: any block may take chunks

@@ -455,12 +455,13 @@ static __device__ __forceinline__ unsigned long long pull_phase(const StepArgs &
 
 // ---------------------------------------------------------------------------
 // Phase B, tiled: the exact E and I sums of a tile of target neurons are formed
-// in shared memory, so no global atomic is issued. Tiles follow population
-// boundaries and hold up to a few thousand targets (16 bytes of counters each),
-// so each source's row into a tile stays a long segment. A tile's work is cut
-// into n_planes parts; blocks take parts from a per-cycle queue (largest
-// first), and part k of a tile stores its sums into accumulator plane k (the
-// LIF phase adds the planes), so parts never write the same word.
+// in shared memory, so no per-event global atomic is issued. Tiles follow
+// population boundaries and hold up to a few thousand targets (16 bytes of
+// counters each), so each source's row into a tile stays a long segment. A
+// tile's work units are cut into parts; blocks take parts from a per-cycle queue
+// (largest first) and, once it is empty, help the parts with the most work
+// left. The first block to finish a piece of a tile stores its sums into the
+// tile's accumulator plane; the others add theirs after that store.
 //
 // The tile's synapses are grouped by (source, delay) and its sources form runs
 // of consecutive ids. A work unit is (run, delay d, 32-source chunk): one lane
@@ -571,7 +572,7 @@ static __device__ __forceinline__ unsigned long long tile_phase(const StepArgs &
         }
         __syncthreads();  // every thread has read s_part / s_best before they are written again
         if (pi < 0) break;
-        const int4 part = a.parts[pi];  // {tile, first unit, end unit, plane}
+        const int4 part = a.parts[pi];  // {tile, first unit, end unit, part within the tile}
         const int q = part.x, u_end = part.z;
         const int tb = a.tile_beg[q], T = a.tile_beg[q + 1] - tb;
         const float sc = a.tile_scale[q];
