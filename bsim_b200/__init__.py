@@ -70,7 +70,7 @@ EXPORTS = [
     "bsim_read_state", "bsim_read_fire_count", "bsim_read_pop_counts", "bsim_get_info", "bsim_get_qexp",
     "bsim_destroy", "bsim_last_error", "bsim_write_state", "bsim_get_stream", "bsim_set_drive",
     "bsim_enable_pop_stats", "bsim_read_pop_info", "bsim_mlp_init", "bsim_mlp_forward", "bsim_mlp_grad",
-    "bsim_mlp_train", "bsim_set_predictor", "bsim_predictor_stats", "bsim_autotune",
+    "bsim_mlp_train", "bsim_set_predictor", "bsim_predictor_stats", "bsim_autotune", "bsim_stall_tile",
 ]
 
 MLP_IN = 9
@@ -111,6 +111,7 @@ def lib():
             "bsim_run": [P, i64],
             "bsim_run_async": [P, i64],
             "bsim_sync": [P],
+            "bsim_stall_tile": [P, i32],
             "bsim_record": [P, i64, i64],
             "bsim_read_raster": [P, P, P, i64, P],
             "bsim_read_state": [P, P, P, P, P],

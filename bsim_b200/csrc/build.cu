@@ -1492,9 +1492,10 @@ static int check_err(Engine &e)
     CK(cudaMemcpy(&err, e.a.err, 4, cudaMemcpyDeviceToHost));
     if (err) {
         static const char *names[] = {"", "row offsets not ascending", "synapse target outside the network",
-                                      "class index or kind out of range", "row offsets do not span the synapses"};
+                                      "class index or kind out of range", "row offsets do not span the synapses",
+                                      "a bounded wait inside the step ran out"};
         std::string m = "device error flag " + std::to_string(err);
-        if (err > 0 && err <= 4) m += std::string(" (") + names[err] + ")";
+        if (err > 0 && err <= 5) m += std::string(" (") + names[err] + ")";
         return fail(BSIM_ERR_DEVICE, m);
     }
     return BSIM_OK;
@@ -1543,6 +1544,20 @@ int bsim_sync(bsim_engine *eh)
     CK(cudaSetDevice(H(eh)->device));
     CK(cudaStreamSynchronize(H(eh)->stream));
     return check_err(*H(eh));
+}
+
+int bsim_stall_tile(bsim_engine *eh, int32_t tile)
+{
+    if (!eh) return fail(BSIM_ERR_ARG, "null engine");
+    Engine &e = *H(eh);
+    if (!e.a.tile_arrive || tile < 0 || tile >= e.a.n_tiles)
+        return fail(BSIM_ERR_ARG, "bsim_stall_tile: the engine has no such tile");
+    CK(cudaSetDevice(e.device));
+    CK(cudaStreamSynchronize(e.stream));
+    // the tile's finisher count of the running cycle (reset by the cycle's last block)
+    const unsigned int one = 1u;
+    CK(cudaMemcpy(e.a.tile_arrive + tile, &one, sizeof(one), cudaMemcpyHostToDevice));
+    return BSIM_OK;
 }
 
 int bsim_run(bsim_engine *eh, int64_t steps)

@@ -191,6 +191,16 @@ int bsim_run(bsim_engine *e, int64_t steps);
 int bsim_run_async(bsim_engine *e, int64_t steps);
 int bsim_sync(bsim_engine *e);
 
+/* Test support for the device error path (no counterpart in the reference, whose
+ * kernels have no bounded waits): marks tile `tile` of a tiled engine as already
+ * claimed by a finisher of the current cycle, so every block that finishes a piece
+ * of it in the next step waits for a store that never comes. The wait gives up
+ * after its bound (about 0.3 s), raises BSIM_DEVERR_TIMEOUT and lets the step end;
+ * bsim_run / bsim_sync then return BSIM_ERR_DEVICE and no later step runs. Every
+ * access stays in bounds and the engine's buffers stay readable. BSIM_ERR_ARG
+ * when the engine has no such tile. */
+int bsim_stall_tile(bsim_engine *e, int32_t tile);
+
 /* Records the fired ids of the next `max_steps` cycles into a device buffer of
  * `capacity` ids (the reference's LOG_DATA GSim.log, SingleGPUSimulator.cu:209-237,
  * without a host sync per step). Calling it again restarts the recording. */

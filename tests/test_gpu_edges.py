@@ -131,3 +131,31 @@ def test_raster_into_caller_buffer():
     again = eng.raster(out=small)
     assert all(np.array_equal(x, y) for x, y in zip(fresh, again)) and not small.any()
     eng.close()
+
+
+def test_bounded_wait_times_out_with_a_device_error():
+    """Failure detection without a GPU fault: a tile whose finisher count is preset
+    (bsim_stall_tile) makes every block that finishes a piece of it wait for a
+    store that never comes. The wait gives up after its bound, the step raises
+    BSIM_DEVERR_TIMEOUT and ends, bsim_run returns BSIM_ERR_DEVICE naming the code,
+    later steps do not run (state unchanged), and the buffers stay readable."""
+    from bsim_b200 import workloads as W
+    import time
+    sp = W.cuba(4, 500, 500, 6, seed=9)
+    eng = B.Engine.generated(sp, DT, opts=B.options(delivery=B.DELIVERY_TILE))
+    eng.run(30)
+    before = eng.state()["v"].copy()
+    with pytest.raises(B.BsimError):
+        B._check(B.lib().bsim_stall_tile(eng._h, eng.info().n_neurons))  # no such tile
+    B._check(B.lib().bsim_stall_tile(eng._h, 0))
+    t0 = time.perf_counter()
+    with pytest.raises(B.BsimError) as err:
+        eng.run(1)
+    assert "bounded wait" in str(err.value) and time.perf_counter() - t0 < 30.0
+    after_fault = eng.state()["v"].copy()
+    assert not np.array_equal(after_fault, before)  # the stalled step itself ran to its end
+    with pytest.raises(B.BsimError):
+        eng.run(5)
+    assert np.array_equal(eng.state()["v"], after_fault)  # nothing ran after the flag
+    assert eng.fire_count().shape == (sp.n_pop * sp.pop_size,)
+    eng.close()
