@@ -592,7 +592,9 @@ def main():
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        # every rank does the same work between collectives (seconds): a rank that dies or
+        # never arrives ends the others' next collective with an error after this bound
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
 
     specs, desc = workload(args.config, 1 + rank)
     deliv = {"push": B.DELIVERY_PUSH, "pull": B.DELIVERY_PULL, "tile": B.DELIVERY_TILE,
