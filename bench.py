@@ -600,7 +600,10 @@ def main():
     deliv = {"push": B.DELIVERY_PUSH, "pull": B.DELIVERY_PULL, "tile": B.DELIVERY_TILE,
              "auto": B.DELIVERY_AUTO}[args.delivery]
     t_build = time.perf_counter()
-    eng = B.Engine.generated(specs, DT, opts=B.options(device=local, delivery=deliv, graph_steps=100))
+    # cycles replayed from CUDA graphs of up to 100 launches; a timed run of K <= 100 cycles is
+    # one graph (captured while the network settles), not K separate launches
+    eng = B.Engine.generated(specs, DT, opts=B.options(device=local, delivery=deliv,
+                                                       graph_steps=max(1, min(100, args.steps))))
     t_build = time.perf_counter() - t_build
     info = eng.info()
     N, S = info.n_neurons, info.n_synapses
