@@ -36,7 +36,9 @@ BYTES_PER_EVENT = 8.0          # int32 target + fp32 weight of one delivered syn
 BYTES_PER_SPIKE = 8.0          # fired id written once, read once
 # Delivery mode per workload when --delivery is not given: the fastest measured on
 # a B200 (1e6-neuron network at ~545 Hz: tiled 0.223 ms per cycle, push ~0.44 ms).
-DEFAULT_DELIVERY = {"plain_1m": "tile"}
+# fastest measured delivery per workload (steady state): tiled on the 1e6-neuron network
+# (-51 % against push) and on the dense one (-4 %)
+DEFAULT_DELIVERY = {"plain_1m": "tile", "dense_1m": "tile"}
 
 
 def workload(name, seed):
