@@ -37,8 +37,9 @@ BYTES_PER_SPIKE = 8.0          # fired id written once, read once
 # Delivery mode per workload when --delivery is not given: the fastest measured on
 # a B200 (1e6-neuron network at ~545 Hz: tiled 0.223 ms per cycle, push ~0.44 ms).
 # fastest measured delivery per workload (steady state): tiled on the 1e6-neuron network
-# (-51 % against push) and on the dense one (-4 %)
-DEFAULT_DELIVERY = {"plain_1m": "tile", "dense_1m": "tile"}
+# (-51 % against push); on the dense one tiled and push are level (2.95-3.11 ms against
+# 3.03-3.08 ms per cycle over several boxes), and push varies less
+DEFAULT_DELIVERY = {"plain_1m": "tile"}
 
 
 def workload(name, seed):

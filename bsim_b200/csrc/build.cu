@@ -702,8 +702,107 @@ __global__ void pair_seg_kernel(const int64_t *pair_base, const uint16_t *pair_d
     }
 }
 
-// tile_pair0: [nt + 1] first pair of each tile (pairs are grouped by tile).
-static int make_pair_seg(Engine &e, int64_t n_pairs, const std::vector<int64_t> &tile_pair0)
+// Entry order inside each (pair, delay) segment of the tiled copy. The sums do
+// not depend on it (exact integers), but the step's shared-memory additions do:
+// a warp adds the first entries of 32 consecutive 16-byte pairs in one atomic
+// instruction and the second entries in the next, and lanes whose counters share
+// a bank serialise. Each segment of up to TILE_SPREAD_MAX entries is reordered so
+// that its first entries (even positions) and its second entries (odd positions)
+// each cycle through distinct banks: every bank's entries are split between the
+// two halves, and each half is laid out bank by bank in rounds. The counter word
+// of an entry is its target (E) or 2 x tile size + target (I), so the bank is
+// that index mod 32. A padding entry stays last (the second entry of its pair).
+#ifndef TILE_BANK_SPREAD
+#define TILE_BANK_SPREAD 1
+#endif
+#define TILE_SPREAD_MAX 256
+#define SPREAD_WARPS 8
+
+static __device__ __forceinline__ int entry_bank(uint2 v, int T)
+{
+    const float w = __uint_as_float(v.y);
+    return (int)((v.x + (w >= 0.0f ? 0u : 2u * (unsigned)T)) & 31u);
+}
+
+__global__ void __launch_bounds__(32 * SPREAD_WARPS) tile_spread_kernel(uint2 *ent, const int64_t *pair_base,
+                                                                      const uint16_t *pair_doff, int64_t n_pairs,
+                                                                      int D, const int64_t *tile_pair0,
+                                                                      const int32_t *tile_size, int32_t nt)
+{
+    __shared__ uint2 s_in[SPREAD_WARPS][TILE_SPREAD_MAX];
+    __shared__ uint16_t s_ord[SPREAD_WARPS][TILE_SPREAD_MAX];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    uint2 *in = s_in[wib];
+    uint16_t *ord = s_ord[wib];
+    for (int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < n_pairs;
+         k += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        int lo = 0, hi = nt - 1;  // the tile whose pair range holds k
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (tile_pair0[mid] <= k) lo = mid;
+            else hi = mid - 1;
+        }
+        const int T = tile_size[lo];
+        for (int d = 0; d < D; d++) {
+            const int64_t b0 = pair_base[k] + pair_doff[k * (D + 1) + d];
+            const int L = (int)(pair_doff[k * (D + 1) + d + 1] - pair_doff[k * (D + 1) + d]);
+            if (L <= 2 || L > TILE_SPREAD_MAX) continue;  // nothing to spread, or kept in target order
+            for (int i = lane; i < L; i += 32) in[i] = ent[b0 + i];
+            __syncwarp();
+            if (lane == 0) {
+                const int pad = in[L - 1].x == TILE_PAD ? 1 : 0;
+                const int nreal = L - pad, half = L / 2;
+                int cnt[32], at[32];
+                for (int b = 0; b < 32; b++) cnt[b] = 0;
+                for (int i = 0; i < nreal; i++) cnt[entry_bank(in[i], T)]++;
+                int run = 0, floors = 0;
+                for (int b = 0; b < 32; b++) {
+                    at[b] = run;
+                    run += cnt[b];
+                    floors += cnt[b] >> 1;
+                }
+                for (int i = 0; i < nreal; i++) ord[at[entry_bank(in[i], T)]++] = (uint16_t)i;  // by bank
+                // each bank's entries: the first ne to the even half, the rest to the odd half;
+                // a bank with an odd count gives its extra entry to the even half while it is short
+                int extra_e = half - floors;
+                int ne[32];
+                for (int b = 0; b < 32; b++) {
+                    ne[b] = cnt[b] >> 1;
+                    if ((cnt[b] & 1) && extra_e > 0) {
+                        ne[b]++;
+                        extra_e--;
+                    }
+                    at[b] -= cnt[b];  // back to the bank's first entry
+                }
+                // each half in rounds over the banks: round r takes the r-th entry of every
+                // bank that has one, so consecutive entries of a round lie in distinct banks
+                int pe = 0, po = 0;
+                for (int r = 0; (pe < half || po < half - pad) && r < TILE_SPREAD_MAX; r++) {
+                    for (int b = 0; b < 32; b++) {
+                        if (r < ne[b]) in[2 * (pe++)].y = ord[at[b] + r];
+                        if (r < cnt[b] - ne[b]) in[2 * (po++) + 1].y = ord[at[b] + ne[b] + r];
+                    }
+                }
+            }
+            __syncwarp();
+            // in[].y now holds, at each output position, the index of the entry that goes there
+            // (the padding entry keeps its own slot); gather, then store
+            uint2 outv[TILE_SPREAD_MAX / 32];
+            for (int i = lane, j = 0; i < L; i += 32, j++) {
+                const bool is_pad = (i == L - 1) && ent[b0 + L - 1].x == TILE_PAD;
+                outv[j] = is_pad ? ent[b0 + i] : ent[b0 + in[i].y];
+            }
+            __syncwarp();
+            for (int i = lane, j = 0; i < L; i += 32, j++) ent[b0 + i] = outv[j];
+            __syncwarp();
+        }
+    }
+}
+
+// tile_pair0: [nt + 1] first pair of each tile (pairs are grouped by tile); tile_beg: [nt + 1]
+// first target of each tile.
+static int make_pair_seg(Engine &e, int64_t n_pairs, const std::vector<int64_t> &tile_pair0,
+                         const std::vector<int32_t> &tile_beg)
 {
     const int32_t nt = (int32_t)tile_pair0.size() - 1;
     for (int32_t q = 0; q < nt && q < (int32_t)e.tile_entries.size(); q++)
@@ -719,6 +818,15 @@ static int make_pair_seg(Engine &e, int64_t n_pairs, const std::vector<int64_t> 
     if (n_pairs > 0 && nt > 0)
         pair_seg_kernel<<<e.sm_count * 4, 256, 0, e.stream>>>(e.a.pair_base, e.a.pair_doff, n_pairs, e.D, d_tp0, nt,
                                                              d_seg0, d_seg);
+    if (TILE_BANK_SPREAD && n_pairs > 0 && nt > 0) {
+        std::vector<int32_t> size(nt);
+        for (int32_t q = 0; q < nt; q++) size[q] = tile_beg[q + 1] - tile_beg[q];
+        int32_t *d_size;
+        TRY(dalloc(e, &d_size, nt));
+        CK(cudaMemcpy(d_size, size.data(), sizeof(int32_t) * nt, cudaMemcpyHostToDevice));
+        tile_spread_kernel<<<e.sm_count * 8, 32 * SPREAD_WARPS, 0, e.stream>>>(
+            const_cast<uint2 *>(e.a.ent), e.a.pair_base, e.a.pair_doff, n_pairs, e.D, d_tp0, d_size, nt);
+    }
     CK(cudaStreamSynchronize(e.stream));
     CK(cudaGetLastError());
     e.a.pair_seg = d_seg;
@@ -851,7 +959,7 @@ static int build_tiles_host(Engine &e, const int32_t *inst, const int32_t *pop, 
     std::vector<int64_t> tile_pair0(nt + 1, (int64_t)pair_base.size());
     for (int32_t q = nt - 1; q >= 0; q--)
         tile_pair0[q] = th.tile_run_off[q] < th.tile_run_off[q + 1] ? th.run_pair0[th.tile_run_off[q]] : tile_pair0[q + 1];
-    TRY(make_pair_seg(e, (int64_t)pair_base.size(), tile_pair0));
+    TRY(make_pair_seg(e, (int64_t)pair_base.size(), tile_pair0, th.tile_beg));
     return upload_tiles(e, th);
 }
 
@@ -1364,7 +1472,7 @@ static int create_generated(const bsim_gen_spec *specs, int32_t ns, float dt, co
         E.a.pair_base = d_pb;
         E.a.pair_doff = d_pd;
         E.a.ent = d_ent;
-        if ((rc = make_pair_seg(E, pairs, tile_pair0))) { free_tmp(); return bail(rc); }
+        if ((rc = make_pair_seg(E, pairs, tile_pair0, tile_beg))) { free_tmp(); return bail(rc); }
         if ((rc = upload_tiles(E, th))) { free_tmp(); return bail(rc); }
     }
     // push rows (not needed when every step uses the tiled copy)
