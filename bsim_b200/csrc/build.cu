@@ -724,16 +724,23 @@ static __device__ __forceinline__ int entry_bank(uint2 v, int T)
     return (int)((v.x + (w >= 0.0f ? 0u : 2u * (unsigned)T)) & 31u);
 }
 
+// One warp per (tile, source) pair, the lanes working on one segment at a time:
+// each entry takes a rank within its bank (shared-memory atomics, so the order
+// inside a bank is arbitrary: it changes nothing), lane b splits bank b's entries
+// between the halves, and each entry computes its place from the 32 banks' counts.
 __global__ void __launch_bounds__(32 * SPREAD_WARPS) tile_spread_kernel(uint2 *ent, const int64_t *pair_base,
                                                                       const uint16_t *pair_doff, int64_t n_pairs,
                                                                       int D, const int64_t *tile_pair0,
                                                                       const int32_t *tile_size, int32_t nt)
 {
-    __shared__ uint2 s_in[SPREAD_WARPS][TILE_SPREAD_MAX];
-    __shared__ uint16_t s_ord[SPREAD_WARPS][TILE_SPREAD_MAX];
+    __shared__ uint8_t s_bank[SPREAD_WARPS][TILE_SPREAD_MAX];
+    __shared__ uint16_t s_rank[SPREAD_WARPS][TILE_SPREAD_MAX];
+    __shared__ uint16_t s_perm[SPREAD_WARPS][TILE_SPREAD_MAX];
+    __shared__ int s_cnt[SPREAD_WARPS][32], s_ne[SPREAD_WARPS][32];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    uint2 *in = s_in[wib];
-    uint16_t *ord = s_ord[wib];
+    uint8_t *bank = s_bank[wib];
+    uint16_t *rank = s_rank[wib], *perm = s_perm[wib];
+    int *cnt = s_cnt[wib], *nes = s_ne[wib];
     for (int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < n_pairs;
          k += ((int64_t)gridDim.x * blockDim.x) >> 5) {
         int lo = 0, hi = nt - 1;  // the tile whose pair range holds k
@@ -747,51 +754,45 @@ __global__ void __launch_bounds__(32 * SPREAD_WARPS) tile_spread_kernel(uint2 *e
             const int64_t b0 = pair_base[k] + pair_doff[k * (D + 1) + d];
             const int L = (int)(pair_doff[k * (D + 1) + d + 1] - pair_doff[k * (D + 1) + d]);
             if (L <= 2 || L > TILE_SPREAD_MAX) continue;  // nothing to spread, or kept in target order
-            for (int i = lane; i < L; i += 32) in[i] = ent[b0 + i];
+            const int pad = ent[b0 + L - 1].x == TILE_PAD ? 1 : 0;
+            const int nreal = L - pad, half = L / 2;
+            cnt[lane] = 0;
             __syncwarp();
-            if (lane == 0) {
-                const int pad = in[L - 1].x == TILE_PAD ? 1 : 0;
-                const int nreal = L - pad, half = L / 2;
-                int cnt[32], at[32];
-                for (int b = 0; b < 32; b++) cnt[b] = 0;
-                for (int i = 0; i < nreal; i++) cnt[entry_bank(in[i], T)]++;
-                int run = 0, floors = 0;
-                for (int b = 0; b < 32; b++) {
-                    at[b] = run;
-                    run += cnt[b];
-                    floors += cnt[b] >> 1;
-                }
-                for (int i = 0; i < nreal; i++) ord[at[entry_bank(in[i], T)]++] = (uint16_t)i;  // by bank
-                // each bank's entries: the first ne to the even half, the rest to the odd half;
-                // a bank with an odd count gives its extra entry to the even half while it is short
-                int extra_e = half - floors;
-                int ne[32];
-                for (int b = 0; b < 32; b++) {
-                    ne[b] = cnt[b] >> 1;
-                    if ((cnt[b] & 1) && extra_e > 0) {
-                        ne[b]++;
-                        extra_e--;
-                    }
-                    at[b] -= cnt[b];  // back to the bank's first entry
-                }
-                // each half in rounds over the banks: round r takes the r-th entry of every
-                // bank that has one, so consecutive entries of a round lie in distinct banks
-                int pe = 0, po = 0;
-                for (int r = 0; (pe < half || po < half - pad) && r < TILE_SPREAD_MAX; r++) {
-                    for (int b = 0; b < 32; b++) {
-                        if (r < ne[b]) in[2 * (pe++)].y = ord[at[b] + r];
-                        if (r < cnt[b] - ne[b]) in[2 * (po++) + 1].y = ord[at[b] + ne[b] + r];
-                    }
-                }
+            for (int i = lane; i < nreal; i += 32) {
+                const int bk = entry_bank(ent[b0 + i], T);
+                bank[i] = (uint8_t)bk;
+                rank[i] = (uint16_t)atomicAdd(&cnt[bk], 1);
             }
             __syncwarp();
-            // in[].y now holds, at each output position, the index of the entry that goes there
-            // (the padding entry keeps its own slot); gather, then store
+            // lane b: how many of bank b's entries go to the first half; banks with an odd
+            // count give their extra entry to the first half while it is short
+            const int c = cnt[lane];
+            int floors = c >> 1;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) floors += __shfl_xor_sync(0xffffffffu, floors, o);
+            const unsigned odd = __ballot_sync(0xffffffffu, c & 1);
+            const int extra = half - floors;
+            nes[lane] = (c >> 1) + (((c & 1) && __popc(odd & ((1u << lane) - 1u)) < extra) ? 1 : 0);
+            __syncwarp();
+            // each half in rounds over the banks: an entry of rank r in its bank's share of a
+            // half goes after every entry of lower rounds and after round r's lower banks
+            for (int i = lane; i < nreal; i += 32) {
+                const int bk = bank[i];
+                const int ne = nes[bk];
+                const bool first = rank[i] < ne;
+                const int r = first ? rank[i] : rank[i] - ne;
+                int pos = 0;
+                for (int b = 0; b < 32; b++) {
+                    const int share = first ? nes[b] : cnt[b] - nes[b];
+                    pos += min(share, r) + ((b < bk && share > r) ? 1 : 0);
+                }
+                perm[first ? 2 * pos : 2 * pos + 1] = (uint16_t)i;
+            }
+            if (pad && lane == 0) perm[L - 1] = (uint16_t)(L - 1);
+            __syncwarp();
+            // gather through registers, then store in place
             uint2 outv[TILE_SPREAD_MAX / 32];
-            for (int i = lane, j = 0; i < L; i += 32, j++) {
-                const bool is_pad = (i == L - 1) && ent[b0 + L - 1].x == TILE_PAD;
-                outv[j] = is_pad ? ent[b0 + i] : ent[b0 + in[i].y];
-            }
+            for (int i = lane, j = 0; i < L; i += 32, j++) outv[j] = ent[b0 + perm[i]];
             __syncwarp();
             for (int i = lane, j = 0; i < L; i += 32, j++) ent[b0 + i] = outv[j];
             __syncwarp();
