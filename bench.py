@@ -66,7 +66,11 @@ def workload(name, seed):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """Clocks, power and throttle reasons sampled while the timed steps run. A timed
+    region of 20 cycles lasts a few milliseconds, so NVML is polled from the host between
+    non-blocking queries of the region's end event (poll_until); where NVML cannot be
+    loaded, nvidia-smi samples every 200 ms instead. Samples are kept as rows of
+    nvidia-smi's csv fields (FIELDS) and summarised by summary()."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -76,10 +80,32 @@ class ClockSampler:
         self.gpu = gpu
         self.proc = None
         self.path = None
+        self.nv = None
+        self.rows = []
+
+    def _nvml_handle(self):
+        nv = self.nv
+        try:
+            import torch
+            uuid = getattr(torch.cuda.get_device_properties(self.gpu), "uuid", None)
+            if uuid is not None:
+                return nv.nvmlDeviceGetHandleByUUID("GPU-" + str(uuid))
+        except Exception:
+            pass
+        return nv.nvmlDeviceGetHandleByIndex(self.gpu)
 
     def __enter__(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.handle = self._nvml_handle()
+            self.sm_max = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
+            return self
+        except Exception:
+            self.nv = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -89,7 +115,38 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def sample(self):
+        """One NVML sample (no-op without NVML)."""
+        if not self.nv:
+            return
+        nv, h = self.nv, self.handle
+        try:
+            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+            rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        except Exception:
+            return
+        bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+        self.rows.append([str(self.gpu), str(sm), str(self.sm_max), "%.2f" % pw, "0x%x" % rs] +
+                         ["Active" if rs & b else "Not Active" for b in bits])
+
+    def poll_until(self, event):
+        """Samples until the CUDA event has completed, then waits for it."""
+        self.sample()
+        while not event.query():
+            self.sample()
+        event.synchronize()
+
     def __exit__(self, *a):
+        if self.nv:
+            with open(self.path, "w") as f:
+                for r in self.rows:
+                    f.write(", ".join(r) + "\n")
+            try:
+                self.nv.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.send_signal(signal.SIGTERM)
             try:
@@ -625,7 +682,7 @@ def main():
         e0.record(stream)
         eng.run_async(args.steps)
         e1.record(stream)
-        e1.synchronize()
+        clk.poll_until(e1)  # clocks sampled while the timed steps run
     eng.sync()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)

@@ -92,3 +92,41 @@ def test_settle_waits_for_the_transient_and_stops_when_flat():
     assert done == 3000                             # already flat: the minimum
     done, _ = bench.settle(_FakeEngine(20000), 3000, 10000)
     assert done == 10000                            # still rising: the maximum
+
+
+def test_clock_sampler_polls_nvml_until_the_event_completes(monkeypatch):
+    """The timed region lasts milliseconds: the sampler polls NVML between non-blocking
+    queries of the end event, so every sample falls inside the region (a fake NVML and a
+    fake event that completes on its fourth query)."""
+    import sys
+    import types
+    calls = {"init": 0, "shutdown": 0}
+    nv = types.SimpleNamespace(
+        NVML_CLOCK_SM=0, nvmlClocksEventReasonHwSlowdown=0x8, nvmlClocksEventReasonHwThermalSlowdown=0x40,
+        nvmlClocksEventReasonSwThermalSlowdown=0x20, nvmlClocksEventReasonSwPowerCap=0x4,
+        nvmlInit=lambda: calls.__setitem__("init", calls["init"] + 1),
+        nvmlShutdown=lambda: calls.__setitem__("shutdown", calls["shutdown"] + 1),
+        nvmlDeviceGetHandleByUUID=lambda u: "h", nvmlDeviceGetHandleByIndex=lambda i: "h",
+        nvmlDeviceGetMaxClockInfo=lambda h, c: 1965, nvmlDeviceGetClockInfo=lambda h, c: 1950,
+        nvmlDeviceGetPowerUsage=lambda h: 812000, nvmlDeviceGetCurrentClocksEventReasons=lambda h: 0x4)
+    monkeypatch.setitem(sys.modules, "pynvml", nv)
+
+    class Event:
+        def __init__(self):
+            self.n = 0
+            self.synced = False
+
+        def query(self):
+            self.n += 1
+            return self.n >= 4
+
+        def synchronize(self):
+            self.synced = True
+
+    ev = Event()
+    with bench.ClockSampler(0) as cs:
+        cs.poll_until(ev)
+    s = cs.summary()
+    assert ev.synced and calls == {"init": 1, "shutdown": 1}
+    assert s["samples"] == 4 and s["sm_mhz"] == 1950.0 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == ["sw_power_cap"] and s["power_w_max"] == 812.0
