@@ -103,6 +103,8 @@ class ClockSampler:
             self.nv = pynvml
             self.handle = self._nvml_handle()
             self.sm_max = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
+            self.sample()  # the first queries take milliseconds: made before the region, not kept
+            self.rows = []
             return self
         except Exception:
             self.nv = None
@@ -131,11 +133,15 @@ class ClockSampler:
         self.rows.append([str(self.gpu), str(sm), str(self.sm_max), "%.2f" % pw, "0x%x" % rs] +
                          ["Active" if rs & b else "Not Active" for b in bits])
 
-    def poll_until(self, event):
-        """Samples until the CUDA event has completed, then waits for it."""
+    def poll_until(self, event, every_s=1e-4):
+        """Samples (at most every `every_s`) until the CUDA event has completed, then waits for it."""
         self.sample()
+        last = time.perf_counter()
         while not event.query():
-            self.sample()
+            now = time.perf_counter()
+            if now - last >= every_s:
+                self.sample()
+                last = now
         event.synchronize()
 
     def __exit__(self, *a):

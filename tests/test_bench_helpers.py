@@ -125,7 +125,7 @@ def test_clock_sampler_polls_nvml_until_the_event_completes(monkeypatch):
 
     ev = Event()
     with bench.ClockSampler(0) as cs:
-        cs.poll_until(ev)
+        cs.poll_until(ev, every_s=0.0)
     s = cs.summary()
     assert ev.synced and calls == {"init": 1, "shutdown": 1}
     assert s["samples"] == 4 and s["sm_mhz"] == 1950.0 and s["sm_max_mhz"] == 1965.0
