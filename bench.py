@@ -56,6 +56,9 @@ def workload(name, seed):
     elif name == "dense_1m":
         specs, _ = W.dense_1m(seed)
         desc = "50 x 20,000 LIF_brian CUBA, ~2 kHz, delays U{1..50}"
+    elif name == "dense_quarter":
+        specs = [W.cuba(50, 5000, 2000, 50, seed, i_max=62.5e-9)]
+        desc = "50 x 5,000 LIF_brian CUBA, ~2 kHz, delays U{1..50} (profiling size of the dense network)"
     elif name.startswith("batched"):
         k = int(name.split("_")[1]) if "_" in name else 256
         specs, _ = W.batched(k, seed)
