@@ -206,9 +206,10 @@ extern "C" int bsim_noalloc_status(void *stream, int32_t *device_error)
     *device_error = err;
     if (err) {
         static const char *names[] = {"", "row offsets not ascending", "synapse target outside the network",
-                                      "class index or kind out of range", "row offsets do not span 0..n_synapses"};
+                                      "class index or kind out of range", "row offsets do not span 0..n_synapses",
+                                      "a bounded wait inside the step ran out"};
         std::string m = "bsim_run_noalloc: device error flag " + std::to_string(err);
-        if (err > 0 && err <= 4) m += std::string(" (") + names[err] + ")";
+        if (err > 0 && err <= 5) m += std::string(" (") + names[err] + ")";
         return record_error(BSIM_ERR_DEVICE, m);
     }
     return BSIM_OK;
