@@ -159,3 +159,46 @@ def test_bounded_wait_times_out_with_a_device_error():
     assert np.array_equal(eng.state()["v"], after_fault)  # nothing ran after the flag
     assert eng.fire_count().shape == (sp.n_pop * sp.pop_size,)
     eng.close()
+
+
+@pytest.mark.parametrize("tile_size", [1024, 256])
+def test_tiled_segment_lengths_around_the_bank_ordering_limit(tile_size):
+    """The tiled copy reorders the entries of each (tile, source, delay) segment of up
+    to 256 entries by shared-memory bank and keeps longer ones in target order. Sources
+    with 1, 2, 3, 255, 256, 257 and 300 targets at one delay (padded to even lengths,
+    excitatory and inhibitory mixed, so both counter halves' banks occur), in one tile
+    and in tiles of 256 targets: spikes, state and events equal the oracle's."""
+    n = 700
+    rng = np.random.default_rng(11)
+    params = lif_params(n, rng.uniform(0.15e-9, 0.35e-9, n), seed=11)
+    params[:7, 9] = 3e-9  # the long-row sources are driven to fire regularly
+    src, dst, w, d = [], [], [], []
+    for s_id, k in enumerate([1, 2, 3, 255, 256, 257, 300]):
+        tg = np.sort(rng.choice(n, k, replace=False))
+        src += [s_id] * k
+        dst += tg.tolist()
+        w += rng.uniform(-6e-11, 9e-11, k).tolist()
+        d += [1 + s_id % 3] * k
+    m = 3000  # background synapses so that the sources fire
+    src += rng.integers(0, n, m).tolist()
+    dst += rng.integers(0, n, m).tolist()
+    w += rng.uniform(-2e-10, 3e-10, m).tolist()
+    d += rng.integers(1, 5, m).tolist()
+    src, dst = np.asarray(src, np.int32), np.asarray(dst, np.int32)
+    w, d = np.asarray(w, np.float32), np.asarray(d, np.int32)
+    steps = 400
+    eng = B.Engine.from_arrays(params, src, dst, w, d, DT,
+                               opts=B.options(delivery=B.DELIVERY_TILE, tile_size=tile_size))
+    eng.record(steps, n * steps)
+    eng.run(steps)
+    ras = eng.raster()
+    ref = oracle.run(params, src, dst, w, d, DT, steps, record_steps=steps, acc_mode=oracle.ACC_FIXED,
+                     qexp=int(eng.qexp()[0]), raster_cap=n * steps)
+    assert sum(len(r) for r in ras) > 0
+    for t in range(steps):
+        assert np.array_equal(ras[t], ref["raster"][t]), t
+    assert np.array_equal(eng.fire_count(), ref["fire_count"])
+    assert np.array_equal(eng.state()["v"], ref["final_state"][:, 0])
+    assert eng.info().events_total == ref["events_per_step"].sum()
+    assert (ref["fire_count"][:7] >= 10).all()  # every long-row source spikes repeatedly
+    eng.close()
